@@ -1,0 +1,301 @@
+#!/usr/bin/env python3
+"""Benchmark of the dynamical-core hot path: zone-cycles/s on B200.
+
+A step is one full RK3 time step of the 3-D moist convection LES
+(128 x 256 x 256 cells, 8 variables: dry air, H2O vapour / liquid / ice,
+momentum, energy) with PPM reconstruction, the HLLC solver, the implicit
+vertical block-tridiagonal correction and the saturation adjustment, i.e.
+the task list of ImplicitHydroTasks.  A zone-cycle is one interior cell
+advanced one step (canoe src/mesh_destroy.cpp:43-53).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank steps its own full block (weak scaling, no data
+collective: the path's blocks are independent between halo exchanges, which
+this build does not do across GPUs).  Rank 0 prints one JSON line.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-cycles/s on 1 B200: mixed+learned vs plain FP64 at stated L2 error"
+UNIT = "zone-cycles/s"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_problem(args, nx2=None, nx3=None):
+    from canoe_b200 import problems
+    return problems.moist3d(nx1=args.nx1, nx2=nx2 or args.nx2, nx3=nx3 or args.nx3,
+                            x1max=16.0e3, x2max=64.0e3 * (nx2 or args.nx2) / 256,
+                            x3max=64.0e3 * (nx3 or args.nx3) / 256)
+
+
+def algorithmic_bytes(nv, ny, ncell):
+    """bytes per launch of each kernel class: inputs read once, outputs written
+    once, interior cells (SURVEY per-unit figures, 8-byte words)."""
+    return {
+        "flux_x1": 16 * nv * ncell,            # read w, write du
+        "flux_x2": 24 * nv * ncell,            # read w, du; write du
+        "flux_x3": 24 * nv * ncell,
+        "update_implicit": (40 * nv + 8 * nv / 3.0) * ncell,  # read w,du,u,u1; write u (+u1)
+        "satadj": 8 * (nv + ny) * ncell,
+        "cons_to_prim": 16 * nv * ncell,
+    }
+
+
+CLASSES = ["flux_x1", "flux_x2", "flux_x3", "update_implicit", "satadj", "cons_to_prim", "dt"]
+LAUNCHES_PER_STEP = {"flux_x1": 3, "flux_x2": 3, "flux_x3": 3, "update_implicit": 3,
+                     "satadj": 1, "cons_to_prim": 3, "dt": 1}
+
+
+def cpu_baseline(args, seconds=12.0, max_steps=20):
+    """The oracle (C++ restatement, OpenMP over all host threads) on a bounded
+    sample of the workload: full 128-level columns on a 48 x 48 horizontal
+    patch, timed for about `seconds`."""
+    from oracle import oracle
+    nthreads = oracle.set_threads(os.cpu_count() or 1)
+    p = make_problem(args, nx2=48, nx3=48)
+    ob = oracle.OracleBlock(p)
+    ncell = p.cfg.nx1 * p.cfg.nx2 * p.cfg.nx3
+    ob.step(-1.0, 1)  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps:
+        ob.step(-1.0, 1)
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": ncell * n / el, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{n} steps of a 128x48x48 patch of the same configuration "
+                      f"({ncell} cells, {el:.1f} s wall)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    cb = cpu_baseline(args, seconds=max(4.0, 2.0 * args.steps), max_steps=max(args.steps, 1))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict(args),
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    return {"workload": f"C2 3-D moist convection LES {args.nx1}x{args.nx2}x{args.nx3}, "
+                        "PPM + HLLC, implicit X1 partial 3x3, saturation adjustment each step",
+            "cells": args.nx1 * args.nx2 * args.nx3, "nv": 8, "rk_stages": 3,
+            "precision": args.precision, "cfl": 0.8,
+            "l2_flush": "inputs larger than L2 (537 MB per state array)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx1", type=int, default=128)
+    ap.add_argument("--nx2", type=int, default=256)
+    ap.add_argument("--nx3", type=int, default=256)
+    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from canoe_b200 import MeshBlock
+    from canoe_b200._abi import check, load
+    lib = load()
+    p = make_problem(args)
+    ncell = p.cfg.nx1 * p.cfg.nx2 * p.cfg.nx3
+    nv, ny = p.nv, p.ny
+    stream = torch.cuda.Stream()
+    blk = MeshBlock(p, graph=True)
+    check(lib.canoe_block_set_stream(blk.h, ctypes.c_void_p(stream.cuda_stream)))
+    launches = 0
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            blk.step()
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        sampler = ClockSampler(local)
+        sampler.start()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            blk.step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        clocks = sampler.stop()
+        launches = args.steps * sum(LAUNCHES_PER_STEP.values())
+        # per-kernel-class timing pass (events between launches, same stream)
+        prof = (ctypes.c_float * 7)()
+        nprof = max(2, min(args.steps, 5))
+        for _ in range(nprof):
+            check(lib.canoe_block_step_profile(blk.h, -1.0, prof, 7))
+        stream.synchronize()
+    err = blk.error_word()
+    t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * ncell * args.steps / (ms * 1e-3)
+
+    # roofline of the dominant kernel class
+    hbm, peak_kind = peaks()
+    abytes = algorithmic_bytes(nv, ny, ncell)
+    per_class = {}
+    for c, name in enumerate(CLASSES):
+        tot = prof[c] / nprof
+        nl = LAUNCHES_PER_STEP[name]
+        per_class[name] = {"ms_per_step": tot, "ms_per_launch": tot / nl}
+        if name in abytes and tot > 0:
+            per_class[name]["gbs"] = abytes[name] / (tot / nl * 1e-3) / 1e9
+    dom = max((n for n in per_class if n in abytes), key=lambda n: per_class[n]["ms_per_step"])
+    ach = per_class[dom]["gbs"]
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(dom)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                "per_kernel": per_class}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        hu = torch.empty(p.u.shape, dtype=torch.float64).pin_memory()
+        hu.numpy()[...] = p.u
+        ho = torch.empty(p.u.shape, dtype=torch.float64).pin_memory()
+        torch.cuda.synchronize()
+        k = args.steps
+        t0 = time.perf_counter()
+        check(lib.canoe_block_set_conserved(blk.h, ctypes.c_void_p(hu.data_ptr())))
+        dtv = ctypes.c_double()
+        for _ in range(k):
+            check(lib.canoe_block_step(blk.h, -1.0))
+            check(lib.canoe_block_new_dt(blk.h, ctypes.byref(dtv)))
+        check(lib.canoe_block_get_conserved(blk.h, ctypes.c_void_p(ho.data_ptr())))
+        el = time.perf_counter() - t0
+        nbytes = hu.numel() * 8
+        e2e = {"value": world * ncell * k / el, "unit": UNIT,
+               "h2d_bytes_per_step": nbytes / k, "d2h_bytes_per_step": nbytes / k + 8,
+               "note": "state uploaded once and downloaded once per K-step run "
+                       "(bytes amortised per step); dt read back every step"}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(args)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded C2 initial state)",
+            "config": config_dict(args), "gpu_launches": launches,
+            "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
+            "error_word": err}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

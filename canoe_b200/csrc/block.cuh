@@ -1,0 +1,74 @@
+// block.cuh -- MeshBlock geometry as seen by the kernels, kernel launchers
+// shared between translation units, and the block object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "physics.cuh"
+
+namespace cb {
+
+// Geometry of one MeshBlock in the reference layout (NV, nc3, nc2, nc1),
+// i fastest (canoe src/interface/hydro.hpp:54-67).
+struct Geom {
+  int ny, nv;
+  int nx1, nx2, nx3, nc1, nc2, nc3;
+  int is, ie, js, je, ks, ke;
+  int f2, f3;
+  int bc[6];
+  int64_t sk;  // stride between k planes  (nc2 * nc1)
+  int64_t sv;  // stride between variables (nc3 * nc2 * nc1)
+  double dx2, dx3;
+  const double *x1f, *x1v, *dx1f;  // device arrays, nc1+1 / nc1 / nc1
+};
+
+// RK3 (SSPRK(3,3), Shu & Osher 1988) register weights per stage:
+// u = g1 u + g2 u1, du weight beta (ImplicitHydroTasks::IntegrateHydro).
+struct Stage {
+  double g1, g2, beta;
+};
+extern const Stage kRK3[3];
+
+// error reporting ----------------------------------------------------------
+void set_error(const std::string &msg);
+int cuda_status(cudaError_t e, const char *what);
+#define CB_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cb::cuda_status(e_, #call); \
+  } while (0)
+
+// kernels launched from the step driver (defined in flux.cu, update.cu,
+// eos.cu).  `dtp` points at the device copy of the step's dt; every kernel
+// multiplies it by the stage's beta so that a step can be captured in a CUDA
+// graph without baking dt in.
+int launch_flux_x1(const Geom &g, const canoe_thermo_t &th, int recon, int rs,
+                   int precision, const double *w, double *du, const double *dtp,
+                   double beta, double *flx_out, cudaStream_t st);
+int launch_flux_x23(int dir, const Geom &g, const canoe_thermo_t &th, int recon,
+                    int rs, int precision, const double *w, double *du,
+                    const double *dtp, double beta, double *flx_out,
+                    cudaStream_t st);
+int launch_update(const Geom &g, const canoe_thermo_t &th, int implicit_flag,
+                  const double *w, double *du, double *u, double *u1,
+                  const double *dtp, const Stage &s, int stage, int mode,
+                  double *scratch, cudaStream_t st);
+int launch_cons_to_prim(const Geom &g, const canoe_thermo_t &th, const double *u,
+                        double *w, uint32_t *err, unsigned long long *dt_acc,
+                        double cfl, int implicit_flag, cudaStream_t st);
+int launch_dt_finalize(double *d_dt, unsigned long long *dt_acc, double cfl,
+                       double fixed_dt, cudaStream_t st);
+int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
+                  double *u, int64_t ncells, int64_t stride, const Geom *g,
+                  const double *t_guess, double *t_out, int32_t *iters,
+                  unsigned long long *stats, cudaStream_t st);
+
+// update modes for launch_update
+enum UpdateMode { kUpdateRK = 0, kUpdateCorrectOnly = 1 };
+
+size_t implicit_scratch_doubles(const Geom &g, int implicit_flag);
+
+}  // namespace cb

@@ -1,0 +1,535 @@
+// capi.cu -- the extern "C" boundary (include/canoe_b200.h): MeshBlock
+// objects that own their device arrays, the RK3 step driver, and the
+// operator-level entry points.  There is no CPU fallback: every entry point
+// runs CUDA kernels or returns an error.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "block.cuh"
+
+namespace cb {
+
+const Stage kRK3[3] = {{0., 1., 1.}, {0.25, 0.75, 0.25}, {2. / 3., 1. / 3., 2. / 3.}};
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int cuda_status(cudaError_t e, const char *what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return CANOE_ERR_CUDA;
+}
+
+namespace {
+
+// operator-level Riemann kernel over (NV, n) face arrays
+template <int NY, int RS, int DIR>
+__global__ void k_riemann_faces(canoe_thermo_t th, const double *__restrict__ wl,
+                                const double *__restrict__ wr,
+                                double *__restrict__ flx, int64_t n) {
+  constexpr int NV = 5 + NY;
+  int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n) return;
+  double a[NV], b[NV], o[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    a[v] = wl[v * n + f];
+    b[v] = wr[v * n + f];
+  }
+  riemann<double, NY, RS, DIR>(th, a, b, o);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) flx[v * n + f] = o[v];
+}
+
+template <int NY, int RS>
+int riemann_faces(const canoe_thermo_t &th, int dir, const double *wl,
+                  const double *wr, double *flx, int64_t n, cudaStream_t st) {
+  unsigned nb = (unsigned)((n + 127) / 128);
+  if (dir == 0) k_riemann_faces<NY, RS, 0><<<nb, 128, 0, st>>>(th, wl, wr, flx, n);
+  else if (dir == 1) k_riemann_faces<NY, RS, 1><<<nb, 128, 0, st>>>(th, wl, wr, flx, n);
+  else k_riemann_faces<NY, RS, 2><<<nb, 128, 0, st>>>(th, wl, wr, flx, n);
+  CB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int riemann_entry(int rs, const canoe_thermo_t *th, int ivx, const double *wl,
+                  const double *wr, double *flx, int64_t n, void *stream) {
+  if (!th || !wl || !wr || !flx || n < 0) {
+    set_error("null pointer or negative size");
+    return CANOE_ERR_ARG;
+  }
+  const int dir = ivx - (1 + th->ny);
+  if (dir < 0 || dir > 2) {
+    set_error("ivx must be IVX, IVY or IVZ");
+    return CANOE_ERR_ARG;
+  }
+  if (n == 0) return 0;
+  cudaStream_t st = (cudaStream_t)stream;
+#define CB_R(NY) \
+  return rs == CANOE_RSOLVER_LMARS ? riemann_faces<NY, 0>(*th, dir, wl, wr, flx, n, st) \
+                                   : riemann_faces<NY, 1>(*th, dir, wl, wr, flx, n, st)
+  switch (th->ny) {
+    case 0: CB_R(0);
+    case 1: CB_R(1);
+    case 2: CB_R(2);
+    case 3: CB_R(3);
+    case 6: CB_R(6);
+    default:
+      set_error("unsupported number of mass-fraction slots");
+      return CANOE_ERR_UNSUPPORTED;
+  }
+#undef CB_R
+}
+
+int check_thermo(const canoe_thermo_t &th) {
+  if (th.ny < 0 || th.ny > CANOE_MAX_NY || th.nvapor < 0 || th.nvapor > th.ny ||
+      th.nvapor > CANOE_MAX_VAPOR) {
+    set_error("invalid species counts in canoe_thermo_t");
+    return CANOE_ERR_ARG;
+  }
+  if (!(th.gammad > 1.) || !(th.rd > 0.)) {
+    set_error("invalid gammad / rd");
+    return CANOE_ERR_ARG;
+  }
+  for (int v = 0; v < th.nvapor; ++v) {
+    for (int s : {th.liq_slot[v], th.ice_slot[v]})
+      if (s != -1 && (s <= th.nvapor || s > th.ny)) {
+        set_error("condensate slot outside the cloud range");
+        return CANOE_ERR_ARG;
+      }
+  }
+  return 0;
+}
+
+}  // namespace
+}  // namespace cb
+
+using namespace cb;
+
+struct canoe_block {
+  canoe_block_config_t cfg;
+  Geom g;
+  canoe_thermo_t th;
+  double *d_u = nullptr, *d_w = nullptr, *d_u1 = nullptr, *d_du = nullptr;
+  double *d_x1f = nullptr, *d_x1v = nullptr, *d_dx1f = nullptr;
+  double *d_scr = nullptr, *d_dt = nullptr;
+  unsigned long long *d_dtacc = nullptr;
+  uint32_t *d_err = nullptr;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph = false;
+  size_t nvals = 0;
+};
+
+static int block_free(canoe_block *b) {
+  if (!b) return 0;
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  for (void *p : {(void *)b->d_u, (void *)b->d_w, (void *)b->d_u1, (void *)b->d_du,
+                  (void *)b->d_x1f, (void *)b->d_x1v, (void *)b->d_dx1f,
+                  (void *)b->d_scr, (void *)b->d_dt, (void *)b->d_dtacc,
+                  (void *)b->d_err})
+    if (p) cudaFree(p);
+  if (b->own_stream && b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return 0;
+}
+
+// optional per-kernel-class timing of a step (CUDA events on b->st)
+struct StepTimer {
+  cudaEvent_t ev[64];
+  int cls[64];
+  int n = 0;
+  int mark(cudaStream_t st, int c) {
+    if (n >= 64) return 0;
+    cls[n] = c;
+    CB_CUDA(cudaEventRecord(ev[n++], st));
+    return 0;
+  }
+};
+
+// one RK3 step, all launches on b->st; fixed_dt <= 0 uses the device dt
+static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullptr) {
+  const Geom &g = b->g;
+  int rc;
+#define CB_MARK(c) \
+  if (tm && (rc = tm->mark(b->st, c))) return rc;
+  CB_MARK(-1);
+  if (fixed_dt > 0.) {
+    // write the fixed dt; the accumulator reset is harmless here
+    if ((rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, fixed_dt, b->st))) return rc;
+  }
+  for (int s = 0; s < 3; ++s) {
+    const Stage &sg = kRK3[s];
+    CB_MARK(-1);
+    if ((rc = launch_flux_x1(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.precision,
+                             b->d_w, b->d_du, b->d_dt, sg.beta, nullptr, b->st)))
+      return rc;
+    CB_MARK(0);
+    if (g.f2 && (rc = launch_flux_x23(1, g, b->th, b->cfg.recon, b->cfg.rsolver,
+                                      b->cfg.precision, b->d_w, b->d_du, b->d_dt, sg.beta,
+                                      nullptr, b->st)))
+      return rc;
+    CB_MARK(1);
+    if (g.f3 && (rc = launch_flux_x23(2, g, b->th, b->cfg.recon, b->cfg.rsolver,
+                                      b->cfg.precision, b->d_w, b->d_du, b->d_dt, sg.beta,
+                                      nullptr, b->st)))
+      return rc;
+    CB_MARK(2);
+    if ((rc = launch_update(g, b->th, b->cfg.implicit_flag, b->d_w, b->d_du, b->d_u,
+                            b->d_u1, b->d_dt, sg, s, kUpdateRK, b->d_scr, b->st)))
+      return rc;
+    CB_MARK(3);
+    if (s == 2 && b->cfg.satadj && b->th.ny > 0) {
+      canoe_satadj_opts_t o{1e-8, 30, 0};
+      const int64_t nin = (int64_t)g.nx1 * g.nx2 * g.nx3;
+      if ((rc = launch_satadj(b->th, o, b->d_u, nin, g.sv, &g, nullptr, nullptr, nullptr,
+                              nullptr, b->st)))
+        return rc;
+      CB_MARK(4);
+    }
+    if ((rc = launch_cons_to_prim(g, b->th, b->d_u, b->d_w, b->d_err,
+                                  s == 2 ? b->d_dtacc : nullptr, b->cfg.cfl,
+                                  b->cfg.implicit_flag, b->st)))
+      return rc;
+    CB_MARK(5);
+  }
+  rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, 0., b->st);
+  if (rc) return rc;
+  CB_MARK(6);
+#undef CB_MARK
+  return 0;
+}
+
+extern "C" {
+
+const char *canoe_version(void) { return "canoe_b200 0.1 (sm_100a)"; }
+
+const char *canoe_last_error(void) { return g_last_error.c_str(); }
+
+int canoe_device_sm_count(int *out) {
+  int dev = 0;
+  CB_CUDA(cudaGetDevice(&dev));
+  CB_CUDA(cudaDeviceGetAttribute(out, cudaDevAttrMultiProcessorCount, dev));
+  return 0;
+}
+
+int canoe_riemann_lmars(const canoe_thermo_t *th, int ivx, const double *wl,
+                        const double *wr, double *flx, int64_t n, void *stream) {
+  return riemann_entry(CANOE_RSOLVER_LMARS, th, ivx, wl, wr, flx, n, stream);
+}
+
+int canoe_riemann_hllc(const canoe_thermo_t *th, int ivx, const double *wl,
+                       const double *wr, double *flx, int64_t n, void *stream) {
+  return riemann_entry(CANOE_RSOLVER_HLLC, th, ivx, wl, wr, flx, n, stream);
+}
+
+int canoe_saturation_adjust(const canoe_thermo_t *th, const canoe_satadj_opts_t *opts,
+                            double *d_u, int64_t ncells, const double *d_t_guess,
+                            double *d_t_out, int32_t *d_iters,
+                            unsigned long long *d_stats, void *stream) {
+  if (!th || !opts || !d_u || ncells < 0) {
+    set_error("null pointer or negative size");
+    return CANOE_ERR_ARG;
+  }
+  if (int rc = check_thermo(*th)) return rc;
+  if (opts->warm && !d_t_guess) {
+    set_error("warm start requested without t_guess");
+    return CANOE_ERR_ARG;
+  }
+  if (!(opts->tol > 0.) || opts->max_iter < 1) {
+    set_error("tol must be > 0 and max_iter >= 1");
+    return CANOE_ERR_ARG;
+  }
+  return launch_satadj(*th, *opts, d_u, ncells, ncells, nullptr, d_t_guess, d_t_out,
+                       d_iters, d_stats, (cudaStream_t)stream);
+}
+
+int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
+  if (!cfg || !out) {
+    set_error("null pointer");
+    return CANOE_ERR_ARG;
+  }
+  *out = nullptr;
+  if (int rc = check_thermo(cfg->thermo)) return rc;
+  if (cfg->nx1 < 4 || cfg->nx2 < 1 || cfg->nx3 < 1 || !cfg->h_x1f) {
+    set_error("block needs nx1 >= 4, nx2, nx3 >= 1 and x1 faces");
+    return CANOE_ERR_ARG;
+  }
+  if (cfg->nx3 > 1 && cfg->nx2 == 1) {
+    set_error("a 3-D block needs nx2 > 1");
+    return CANOE_ERR_ARG;
+  }
+  if (cfg->recon != CANOE_RECON_PLM && cfg->recon != CANOE_RECON_PPM) {
+    set_error("recon must be 2 (PLM) or 3 (PPM)");
+    return CANOE_ERR_ARG;
+  }
+  if (cfg->rsolver != CANOE_RSOLVER_LMARS && cfg->rsolver != CANOE_RSOLVER_HLLC) {
+    set_error("unknown Riemann solver");
+    return CANOE_ERR_ARG;
+  }
+  if (cfg->precision != CANOE_FP64) {
+    set_error("only the FP64 path is available in this build");
+    return CANOE_ERR_UNSUPPORTED;
+  }
+  for (int i = 0; i < cfg->nx1; ++i)
+    if (!(cfg->h_x1f[i + 1] > cfg->h_x1f[i])) {
+      set_error("x1 faces must increase");
+      return CANOE_ERR_ARG;
+    }
+  if (cfg->recon == CANOE_RECON_PPM) {
+    double d0 = cfg->h_x1f[1] - cfg->h_x1f[0];
+    for (int i = 1; i < cfg->nx1; ++i)
+      if (std::fabs((cfg->h_x1f[i + 1] - cfg->h_x1f[i]) - d0) > 1e-9 * d0) {
+        set_error("PPM needs a uniform x1 grid");
+        return CANOE_ERR_UNSUPPORTED;
+      }
+  }
+  canoe_block *b = new canoe_block();
+  b->cfg = *cfg;
+  b->cfg.h_x1f = nullptr;
+  b->th = cfg->thermo;
+  Geom &g = b->g;
+  g.ny = b->th.ny;
+  g.nv = 5 + g.ny;
+  g.nx1 = cfg->nx1;
+  g.nx2 = cfg->nx2;
+  g.nx3 = cfg->nx3;
+  g.f2 = cfg->nx2 > 1;
+  g.f3 = cfg->nx3 > 1;
+  g.nc1 = g.nx1 + 2 * NG;
+  g.nc2 = g.f2 ? g.nx2 + 2 * NG : 1;
+  g.nc3 = g.f3 ? g.nx3 + 2 * NG : 1;
+  g.is = NG;
+  g.ie = NG + g.nx1 - 1;
+  g.js = g.f2 ? NG : 0;
+  g.je = g.js + g.nx2 - 1;
+  g.ks = g.f3 ? NG : 0;
+  g.ke = g.ks + g.nx3 - 1;
+  for (int q = 0; q < 6; ++q) g.bc[q] = cfg->bc[q];
+  g.sk = (int64_t)g.nc2 * g.nc1;
+  g.sv = (int64_t)g.nc3 * g.sk;
+  g.dx2 = cfg->dx2;
+  g.dx3 = cfg->dx3;
+  // x1 geometry with mirrored ghost faces
+  std::vector<double> xf(g.nc1 + 1), xv(g.nc1), dx(g.nc1);
+  for (int i = 0; i <= g.nx1; ++i) xf[g.is + i] = cfg->h_x1f[i];
+  for (int q = 1; q <= NG; ++q) {
+    xf[g.is - q] = 2. * xf[g.is] - xf[g.is + q];
+    xf[g.ie + 1 + q] = 2. * xf[g.ie + 1] - xf[g.ie + 1 - q];
+  }
+  for (int i = 0; i < g.nc1; ++i) {
+    xv[i] = 0.5 * (xf[i] + xf[i + 1]);
+    dx[i] = xf[i + 1] - xf[i];
+  }
+  b->nvals = (size_t)g.nv * g.sv;
+  const size_t bytes = b->nvals * sizeof(double);
+  int rc = 0;
+  auto fail = [&](cudaError_t e, const char *w) {
+    rc = cuda_status(e, w);
+    block_free(b);
+    return rc;
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&b->d_u, bytes))) return fail(e, "cudaMalloc u");
+  if ((e = cudaMalloc(&b->d_w, bytes))) return fail(e, "cudaMalloc w");
+  if ((e = cudaMalloc(&b->d_u1, bytes))) return fail(e, "cudaMalloc u1");
+  if ((e = cudaMalloc(&b->d_du, bytes))) return fail(e, "cudaMalloc du");
+  if ((e = cudaMalloc(&b->d_x1f, (g.nc1 + 1) * sizeof(double)))) return fail(e, "cudaMalloc x1f");
+  if ((e = cudaMalloc(&b->d_x1v, g.nc1 * sizeof(double)))) return fail(e, "cudaMalloc x1v");
+  if ((e = cudaMalloc(&b->d_dx1f, g.nc1 * sizeof(double)))) return fail(e, "cudaMalloc dx1f");
+  if ((e = cudaMalloc(&b->d_dt, 2 * sizeof(double)))) return fail(e, "cudaMalloc dt");
+  if ((e = cudaMalloc(&b->d_dtacc, sizeof(unsigned long long)))) return fail(e, "cudaMalloc dtacc");
+  if ((e = cudaMalloc(&b->d_err, sizeof(uint32_t)))) return fail(e, "cudaMalloc err");
+  size_t ns = implicit_scratch_doubles(g, cfg->implicit_flag);
+  if (ns && (e = cudaMalloc(&b->d_scr, ns * sizeof(double)))) return fail(e, "cudaMalloc scratch");
+  if ((e = cudaMemset(b->d_u, 0, bytes))) return fail(e, "cudaMemset u");
+  if ((e = cudaMemset(b->d_w, 0, bytes))) return fail(e, "cudaMemset w");
+  if ((e = cudaMemset(b->d_u1, 0, bytes))) return fail(e, "cudaMemset u1");
+  if ((e = cudaMemset(b->d_du, 0, bytes))) return fail(e, "cudaMemset du");
+  if ((e = cudaMemset(b->d_err, 0, sizeof(uint32_t)))) return fail(e, "cudaMemset err");
+  unsigned long long inf = 0x7ff0000000000000ULL;
+  double zero2[2] = {0., 0.};
+  if ((e = cudaMemcpy(b->d_dtacc, &inf, sizeof(inf), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  if ((e = cudaMemcpy(b->d_dt, zero2, sizeof(zero2), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  if ((e = cudaMemcpy(b->d_x1f, xf.data(), xf.size() * sizeof(double), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  if ((e = cudaMemcpy(b->d_x1v, xv.data(), xv.size() * sizeof(double), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  if ((e = cudaMemcpy(b->d_dx1f, dx.data(), dx.size() * sizeof(double), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking))) return fail(e, "stream");
+  b->own_stream = true;
+  g.x1f = b->d_x1f;
+  g.x1v = b->d_x1v;
+  g.dx1f = b->d_dx1f;
+  *out = b;
+  return 0;
+}
+
+int canoe_block_destroy(canoe_block_t b) {
+  if (b && b->st) cudaStreamSynchronize(b->st);
+  return block_free(b);
+}
+
+int canoe_block_dims(canoe_block_t b, int32_t *nv, int32_t *nc1, int32_t *nc2,
+                     int32_t *nc3) {
+  if (!b) return CANOE_ERR_ARG;
+  if (nv) *nv = b->g.nv;
+  if (nc1) *nc1 = b->g.nc1;
+  if (nc2) *nc2 = b->g.nc2;
+  if (nc3) *nc3 = b->g.nc3;
+  return 0;
+}
+
+int canoe_block_set_stream(canoe_block_t b, void *stream) {
+  if (!b) return CANOE_ERR_ARG;
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  if (b->own_stream) cudaStreamDestroy(b->st);
+  b->st = (cudaStream_t)stream;
+  b->own_stream = false;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return 0;
+}
+
+int canoe_block_set_conserved(canoe_block_t b, const double *h_u) {
+  if (!b || !h_u) return CANOE_ERR_ARG;
+  CB_CUDA(cudaMemcpyAsync(b->d_u, h_u, b->nvals * sizeof(double), cudaMemcpyHostToDevice, b->st));
+  if (int rc = launch_cons_to_prim(b->g, b->th, b->d_u, b->d_w, b->d_err, b->d_dtacc,
+                                   b->cfg.cfl, b->cfg.implicit_flag, b->st))
+    return rc;
+  if (int rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, 0., b->st)) return rc;
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_block_get_conserved(canoe_block_t b, double *h_u) {
+  if (!b || !h_u) return CANOE_ERR_ARG;
+  CB_CUDA(cudaMemcpyAsync(h_u, b->d_u, b->nvals * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_block_get_primitive(canoe_block_t b, double *h_w) {
+  if (!b || !h_w) return CANOE_ERR_ARG;
+  CB_CUDA(cudaMemcpyAsync(h_w, b->d_w, b->nvals * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_block_device_ptrs(canoe_block_t b, double **d_u, double **d_w) {
+  if (!b) return CANOE_ERR_ARG;
+  if (d_u) *d_u = b->d_u;
+  if (d_w) *d_w = b->d_w;
+  return 0;
+}
+
+int canoe_block_calculate_fluxes(canoe_block_t b, double *f1, double *f2, double *f3) {
+  if (!b || !f1 || (b->g.f2 && !f2) || (b->g.f3 && !f3)) {
+    set_error("null flux array");
+    return CANOE_ERR_ARG;
+  }
+  const Geom &g = b->g;
+  int rc;
+  if ((rc = launch_flux_x1(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.precision, b->d_w,
+                           b->d_du, b->d_dt, 1., f1, b->st)))
+    return rc;
+  if (g.f2 && (rc = launch_flux_x23(1, g, b->th, b->cfg.recon, b->cfg.rsolver,
+                                    b->cfg.precision, b->d_w, b->d_du, b->d_dt, 1., f2, b->st)))
+    return rc;
+  if (g.f3 && (rc = launch_flux_x23(2, g, b->th, b->cfg.recon, b->cfg.rsolver,
+                                    b->cfg.precision, b->d_w, b->d_du, b->d_dt, 1., f3, b->st)))
+    return rc;
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt) {
+  if (!b || !d_du || !(dt > 0.)) {
+    set_error("null du or non-positive dt");
+    return CANOE_ERR_ARG;
+  }
+  if (!(b->cfg.implicit_flag & 1)) return 0;
+  // the solve reads dt through the device dt slot: use slot 1 as a scratch
+  CB_CUDA(cudaMemcpyAsync(b->d_dt + 1, &dt, sizeof(double), cudaMemcpyHostToDevice, b->st));
+  Stage s{0., 1., 1.};
+  int rc = launch_update(b->g, b->th, b->cfg.implicit_flag, b->d_w, d_du, b->d_u, b->d_u1,
+                         b->d_dt + 1, s, 1, kUpdateCorrectOnly, b->d_scr, b->st);
+  if (rc) return rc;
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_block_use_graph(canoe_block_t b, int on) {
+  if (!b) return CANOE_ERR_ARG;
+  b->graph = on != 0;
+  return 0;
+}
+
+int canoe_block_step(canoe_block_t b, double dt) {
+  if (!b) return CANOE_ERR_ARG;
+  if (b->graph && !(dt > 0.)) {
+    if (!b->gexec) {
+      cudaGraph_t graph;
+      CB_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+      int rc = step_launches(b, 0.);
+      cudaError_t e = cudaStreamEndCapture(b->st, &graph);
+      if (rc) return rc;
+      if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+      e = cudaGraphInstantiate(&b->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+    }
+    CB_CUDA(cudaGraphLaunch(b->gexec, b->st));
+    return 0;
+  }
+  return step_launches(b, dt);
+}
+
+int canoe_block_step_profile(canoe_block_t b, double dt, float *ms, int nclass) {
+  if (!b || !ms || nclass < 7) {
+    set_error("canoe_block_step_profile needs ms[7]");
+    return CANOE_ERR_ARG;
+  }
+  StepTimer tm;
+  for (int q = 0; q < 64; ++q) CB_CUDA(cudaEventCreate(&tm.ev[q]));
+  int rc = step_launches(b, dt, &tm);
+  if (!rc) {
+    CB_CUDA(cudaEventSynchronize(tm.ev[tm.n - 1]));
+    for (int q = 1; q < tm.n; ++q) {
+      float t = 0.f;
+      CB_CUDA(cudaEventElapsedTime(&t, tm.ev[q - 1], tm.ev[q]));
+      if (tm.cls[q] >= 0 && tm.cls[q] < nclass) ms[tm.cls[q]] += t;
+    }
+  }
+  for (int q = 0; q < 64; ++q) cudaEventDestroy(tm.ev[q]);
+  return rc;
+}
+
+int canoe_block_synchronize(canoe_block_t b) {
+  if (!b) return CANOE_ERR_ARG;
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_block_new_dt(canoe_block_t b, double *dt_out) {
+  if (!b || !dt_out) return CANOE_ERR_ARG;
+  CB_CUDA(cudaMemcpyAsync(dt_out, b->d_dt, sizeof(double), cudaMemcpyDeviceToHost, b->st));
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_block_error_word(canoe_block_t b, uint32_t *bits) {
+  if (!b || !bits) return CANOE_ERR_ARG;
+  CB_CUDA(cudaMemcpyAsync(bits, b->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, b->st));
+  CB_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), b->st));
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,426 @@
+// eos.cu -- cons -> prim over the whole block (ghost cells included), the
+// CFL time step, and the saturation adjustment.
+//
+// k_cons_to_prim: every cell, interior or ghost, converts the conserved state
+//   of its source cell (itself, or its reflected / periodic / outflow image
+//   in the interior) and flips the normal velocity for reflecting walls.
+//   This is EquationOfState::ConservedToPrimitive (snapy "U->W", canoe
+//   src/snap/eos/ideal_moist_hydro.cpp:47-58) and the Athena boundary
+//   conditions in one pass; interior cells also feed the device error word
+//   (canoe src/checks.cpp:53-149) and the CFL minimum of
+//   Hydro::NewBlockTimeStep (patches/21.new_blockdt.patch:20-40).
+// k_satadj: the isochoric, isoenergetic saturation adjustment of
+//   ImplicitHydroTasks::UpdateAllConserved (src/tasklist/implicit_hydro_tasks.
+//   cpp:290-313), Newton on T with a bracketed fallback.
+#include <cuda_runtime.h>
+
+#include "block.cuh"
+
+namespace cb {
+
+namespace {
+
+__device__ __forceinline__ int map_ghost(int i, int lo, int hi, int n, int bcl,
+                                         int bch, bool &flip) {
+  if (i < lo) {
+    if (bcl == CANOE_BC_REFLECT) {
+      flip = !flip;
+      return 2 * lo - 1 - i;
+    }
+    if (bcl == CANOE_BC_PERIODIC) return i + n;
+    return lo;
+  }
+  if (i > hi) {
+    if (bch == CANOE_BC_REFLECT) {
+      flip = !flip;
+      return 2 * hi + 1 - i;
+    }
+    if (bch == CANOE_BC_PERIODIC) return i - n;
+    return hi;
+  }
+  return i;
+}
+
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+
+template <int NY>
+__global__ void __launch_bounds__(256)
+    k_cons_to_prim(Geom g, canoe_thermo_t th, const double *__restrict__ u,
+                   double *__restrict__ w, uint32_t *err,
+                   unsigned long long *dt_acc, double cfl, int imp) {
+  using S = Slots<NY>;
+  constexpr int NV = S::NV;
+  const int64_t total = (int64_t)g.nc3 * g.sk;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double dtc = __longlong_as_double(0x7ff0000000000000LL);
+  uint32_t bits = 0;
+  if (t < total) {
+    const int i = (int)(t % g.nc1);
+    const int j = (int)((t / g.nc1) % g.nc2);
+    const int k = (int)(t / g.sk);
+    bool f1 = false, f2 = false, f3 = false;
+    const int si = map_ghost(i, g.is, g.ie, g.nx1, g.bc[0], g.bc[1], f1);
+    const int sj = g.f2 ? map_ghost(j, g.js, g.je, g.nx2, g.bc[2], g.bc[3], f2) : j;
+    const int sk = g.f3 ? map_ghost(k, g.ks, g.ke, g.nx3, g.bc[4], g.bc[5], f3) : k;
+    const int64_t src = (int64_t)sk * g.sk + (int64_t)sj * g.nc1 + si;
+    double uc[NV], wc[NV];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) uc[n] = u[n * g.sv + src];
+    cons_to_prim<NY>(th, uc, wc);
+    if (f1) wc[S::IVX] = -wc[S::IVX];
+    if (f2) wc[S::IVY] = -wc[S::IVY];
+    if (f3) wc[S::IVZ] = -wc[S::IVZ];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) w[n * g.sv + t] = wc[n];
+    const bool interior = si == i && sj == j && sk == k;
+    if (interior) {
+      double rho = wc[0], p = wc[S::IPR];
+      if (!(rho > 0.)) bits |= (rho != rho) ? CANOE_EBIT_NAN : CANOE_EBIT_NEG_DENSITY;
+      if (!(p > 0.)) bits |= (p != p) ? CANOE_EBIT_NAN : CANOE_EBIT_NEG_PRESSURE;
+      if (dt_acc) {
+        double cs = sound_speed<double, NY>(th, wc);
+        double d1 = g.dx1f[i];
+        if ((imp & 1) && g.nx2 > 1)
+          d1 /= cfl * fabs(wc[S::IVX]);
+        else
+          d1 /= (fabs(wc[S::IVX]) + cs);
+        dtc = d1;
+        if (g.f2) dtc = fmin(dtc, g.dx2 / (fabs(wc[S::IVY]) + cs));
+        if (g.f3) dtc = fmin(dtc, g.dx3 / (fabs(wc[S::IVZ]) + cs));
+      }
+    }
+  }
+  // warp reductions
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+    bits |= __shfl_xor_sync(0xffffffffu, bits, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (bits) atomicOr(err, bits);
+    if (dt_acc && dtc < __longlong_as_double(0x7ff0000000000000LL)) atomicMin(dt_acc, dbits(dtc));
+  }
+}
+
+__global__ void k_dt_finalize(double *d_dt, unsigned long long *acc, double cfl,
+                              double fixed_dt) {
+  if (fixed_dt > 0.)
+    d_dt[0] = fixed_dt;
+  else
+    d_dt[0] = cfl * __longlong_as_double((long long)*acc);
+  *acc = 0x7ff0000000000000ULL;
+}
+
+// ---------------------------------------------------------------------------
+// saturation adjustment (model and algorithm as documented in the header of
+// this function's host entry point, canoe_saturation_adjust)
+
+template <int NY>
+struct SatCell {
+  double rho, ie, qd;
+  double qt[NY > 0 ? NY : 1];
+  double qinert[NY + 1];
+};
+
+template <int NY>
+__device__ __forceinline__ void sat_eval(const canoe_thermo_t &th, const SatCell<NY> &c,
+                                         double T, int fv, int fphase, double &f,
+                                         double &fp, double *q) {
+  const double cvd = th.rd / (th.gammad - 1.);
+#pragma unroll
+  for (int n = 0; n <= NY; ++n) q[n] = c.qinert[n];
+  double cvs = c.qd, lat = 0., dlat = 0.;
+#pragma unroll
+  for (int n = 1; n <= NY; ++n)
+    if (c.qinert[n] != 0.) {
+      cvs += c.qinert[n] * (1. + th.cv_ratio_m1[n - 1]);
+      lat += c.qinert[n] * th.u0[n - 1];
+    }
+#pragma unroll
+  for (int v = 0; v < (NY > 0 ? NY : 1); ++v) {
+    if (v >= th.nvapor) break;
+    const int vs = 1 + v, ls = th.liq_slot[v], ss = th.ice_slot[v];
+    if (ls < 0 && ss < 0) {
+#pragma unroll
+      for (int n = 1; n <= NY; ++n)
+        if (n == vs) q[n] = c.qt[v];
+      cvs += c.qt[v] * (1. + th.cv_ratio_m1[vs - 1]);
+      continue;
+    }
+    bool liquid = (ss < 0) || (ls >= 0 && T >= th.t3[v]);
+    if (v == fv) liquid = (fphase == 0);
+    const int cs = liquid ? ls : ss;
+    const double beta = liquid ? th.beta_l[v] : th.beta_s[v];
+    const double delta = liquid ? th.delta_l[v] : th.delta_s[v];
+    const double rv = th.rd * (1. + th.inv_mu_ratio_m1[vs - 1]);
+    const double lnps =
+        log(th.p3[v]) + beta * (1. - th.t3[v] / T) - delta * log(T / th.t3[v]);
+    const double qs = exp(lnps) / (c.rho * rv * T);
+    double qv, qc, dqv;
+    if (qs < c.qt[v]) {
+      qv = qs;
+      qc = c.qt[v] - qs;
+      dqv = qs * (beta * th.t3[v] / (T * T) - delta / T - 1. / T);
+    } else {
+      qv = c.qt[v];
+      qc = 0.;
+      dqv = 0.;
+    }
+    const double cvv = 1. + th.cv_ratio_m1[vs - 1];
+    const double cvc = 1. + th.cv_ratio_m1[cs - 1];
+#pragma unroll
+    for (int n = 1; n <= NY; ++n) {
+      if (n == vs) q[n] = qv;
+      if (n == cs) q[n] += qc;
+    }
+    cvs += qv * cvv + qc * cvc;
+    lat += qc * th.u0[cs - 1];
+    dlat += dqv * (cvd * cvv * T - cvd * cvc * T - th.u0[cs - 1]);
+  }
+  f = c.rho * (cvd * cvs * T + lat) - c.ie;
+  fp = c.rho * (cvd * cvs + dlat);
+}
+
+// returns iterations; flags bit0 fallback, bit1 not converged
+template <int NY>
+__device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
+                        double *uc, double t_guess, double &t_out, int &flags) {
+  using S = Slots<NY>;
+  const double cvd = th.rd / (th.gammad - 1.);
+  SatCell<NY> c;
+  c.rho = uc[0];
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) c.rho += uc[n];
+  const double m1 = uc[S::IVX], m2 = uc[S::IVY], m3 = uc[S::IVZ];
+  const double ke = 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / c.rho;
+  c.ie = uc[S::IPR] - ke;
+  double q[NY + 1];
+  double qsum = 0.;
+  q[0] = 0.;
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) {
+    q[n] = uc[n] / c.rho;
+    qsum += q[n];
+  }
+  c.qd = 1. - qsum;
+  bool member[NY + 1];
+#pragma unroll
+  for (int n = 0; n <= NY; ++n) {
+    c.qinert[n] = 0.;
+    member[n] = false;
+  }
+#pragma unroll
+  for (int v = 0; v < (NY > 0 ? NY : 1); ++v) {
+    if (v >= th.nvapor) break;
+    double qt = 0.;
+#pragma unroll
+    for (int n = 1; n <= NY; ++n)
+      if (n == 1 + v) {
+        qt = q[n];
+        member[n] = true;
+      }
+    const int ls = th.liq_slot[v], ss = th.ice_slot[v];
+#pragma unroll
+    for (int n = 1; n <= NY; ++n)
+      if (ls > 0 && n == ls) {
+        qt += q[n];
+        member[n] = true;
+      }
+#pragma unroll
+    for (int n = 1; n <= NY; ++n)
+      if (ss > 0 && n == ss) {
+        qt += q[n];
+        member[n] = true;
+      }
+    c.qt[v] = qt;
+  }
+#pragma unroll
+  for (int n = 1; n <= NY; ++n)
+    if (!member[n]) c.qinert[n] = q[n];
+  double cvs = c.qd, lat = 0.;
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) {
+    cvs += q[n] * (1. + th.cv_ratio_m1[n - 1]);
+    lat += q[n] * th.u0[n - 1];
+  }
+  const double t_cold = (c.ie / c.rho - lat) / (cvd * cvs);
+
+  int iters = 0;
+  bool fallback = false, converged = false;
+  double T = t_cold;
+  if (o.warm && isfinite(t_guess) && t_guess > 1. && t_guess < 1.e4) T = t_guess;
+  double fprev = __longlong_as_double(0x7ff0000000000000LL);
+  double f, fp;
+  double qn[NY + 1];
+  for (int it = 0; it < o.max_iter; ++it) {
+    sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+    if (!(fabs(f) < fprev) && it > 0) {
+      fallback = true;
+      break;
+    }
+    const double dT = -f / fp;
+    T += dT;
+    iters++;
+    fprev = fabs(f);
+    if (fabs(dT) < o.tol) {
+      converged = true;
+      break;
+    }
+  }
+  if (!converged) {
+    fallback = true;
+    double lo = 1., hi = 1.e4;
+    if (!(T > lo && T < hi)) T = t_cold;
+    for (int it = 0; it < 200; ++it) {
+      sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+      if (f < 0.) lo = T;
+      else hi = T;
+      double tn = T - f / fp;
+      if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
+      const double dT = tn - T;
+      T = tn;
+      iters++;
+      if (fabs(dT) < o.tol || hi - lo < o.tol) {
+        converged = true;
+        break;
+      }
+    }
+  }
+  sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+  // root on a liquid / ice jump at t3: split the condensate
+#pragma unroll
+  for (int v = 0; v < (NY > 0 ? NY : 1); ++v) {
+    if (v >= th.nvapor) break;
+    const int ls = th.liq_slot[v], ss = th.ice_slot[v];
+    if (ls < 0 || ss < 0) continue;
+    if (fabs(T - th.t3[v]) > 2. * o.tol + 1e-12 * th.t3[v]) continue;
+    double fl, fs, fpl, fps;
+    double ql[NY + 1], qs_[NY + 1];
+    sat_eval<NY>(th, c, th.t3[v], v, 0, fl, fpl, ql);
+    sat_eval<NY>(th, c, th.t3[v], v, 1, fs, fps, qs_);
+    if ((fl > 0.) == (fs > 0.)) continue;
+    const double x = -fs / (fl - fs);
+    T = th.t3[v];
+    double qc = 0.;
+#pragma unroll
+    for (int n = 1; n <= NY; ++n)
+      if (n == ls) qc = ql[n];
+#pragma unroll
+    for (int n = 0; n <= NY; ++n) {
+      qn[n] = ql[n];
+      if (n == ls) qn[n] = x * qc;
+      if (n == ss) qn[n] = qc - x * qc;
+    }
+    break;
+  }
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) uc[n] = qn[n] * c.rho;
+  t_out = T;
+  flags = (fallback ? 1 : 0) | (converged ? 0 : 2);
+  return iters;
+}
+
+template <int NY>
+__global__ void __launch_bounds__(256)
+    k_satadj(canoe_thermo_t th, canoe_satadj_opts_t o, double *__restrict__ u,
+             int64_t ncells, int64_t stride, Geom g, int use_geom,
+             const double *__restrict__ t_guess, double *__restrict__ t_out,
+             int32_t *__restrict__ iters, unsigned long long *stats) {
+  using S = Slots<NY>;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int it = 0, fl = 0;
+  bool active = t < ncells;
+  if (active) {
+    int64_t off = t;
+    if (use_geom) {
+      const int i = g.is + (int)(t % g.nx1);
+      const int64_t r = t / g.nx1;
+      const int j = g.js + (int)(r % g.nx2), k = g.ks + (int)(r / g.nx2);
+      off = (int64_t)k * g.sk + (int64_t)j * g.nc1 + i;
+    }
+    double uc[S::NV];
+#pragma unroll
+    for (int n = 0; n < S::NV; ++n) uc[n] = u[n * stride + off];
+    double T;
+    it = sat_cell<NY>(th, o, uc, t_guess ? t_guess[t] : 0., T, fl);
+#pragma unroll
+    for (int n = 1; n <= NY; ++n) u[n * stride + off] = uc[n];
+    if (t_out) t_out[t] = T;
+    if (iters) iters[t] = it;
+  }
+  if (stats) {
+    unsigned long long a = active ? 1ull : 0ull, b = (unsigned long long)it,
+                       c = (fl & 1) ? 1ull : 0ull, d = (fl & 2) ? 1ull : 0ull;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, s);
+      b += __shfl_xor_sync(0xffffffffu, b, s);
+      c += __shfl_xor_sync(0xffffffffu, c, s);
+      d += __shfl_xor_sync(0xffffffffu, d, s);
+    }
+    if ((threadIdx.x & 31) == 0 && a) {
+      atomicAdd(&stats[0], a);
+      atomicAdd(&stats[1], b);
+      if (c) atomicAdd(&stats[2], c);
+      if (d) atomicAdd(&stats[3], d);
+    }
+  }
+}
+
+}  // namespace
+
+int launch_cons_to_prim(const Geom &g, const canoe_thermo_t &th, const double *u,
+                        double *w, uint32_t *err, unsigned long long *dt_acc,
+                        double cfl, int imp, cudaStream_t st) {
+  const int64_t total = (int64_t)g.nc3 * g.sk;
+  const unsigned nb = (unsigned)((total + 255) / 256);
+  switch (th.ny) {
+    case 0: k_cons_to_prim<0><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
+    case 1: k_cons_to_prim<1><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
+    case 2: k_cons_to_prim<2><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
+    case 3: k_cons_to_prim<3><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
+    case 6: k_cons_to_prim<6><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
+    default:
+      set_error("unsupported number of mass-fraction slots");
+      return CANOE_ERR_UNSUPPORTED;
+  }
+  CB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_dt_finalize(double *d_dt, unsigned long long *acc, double cfl,
+                       double fixed_dt, cudaStream_t st) {
+  k_dt_finalize<<<1, 1, 0, st>>>(d_dt, acc, cfl, fixed_dt);
+  CB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o, double *u,
+                  int64_t ncells, int64_t stride, const Geom *g, const double *t_guess,
+                  double *t_out, int32_t *iters, unsigned long long *stats,
+                  cudaStream_t st) {
+  if (ncells <= 0) return 0;
+  Geom gg{};
+  if (g) gg = *g;
+  const unsigned nb = (unsigned)((ncells + 255) / 256);
+  const int ug = g ? 1 : 0;
+#define CB_SAT(NY) \
+  k_satadj<NY><<<nb, 256, 0, st>>>(th, o, u, ncells, stride, gg, ug, t_guess, t_out, iters, stats)
+  switch (th.ny) {
+    case 1: CB_SAT(1); break;
+    case 2: CB_SAT(2); break;
+    case 3: CB_SAT(3); break;
+    case 6: CB_SAT(6); break;
+    case 0: return 0;
+    default:
+      set_error("unsupported number of mass-fraction slots");
+      return CANOE_ERR_UNSUPPORTED;
+  }
+#undef CB_SAT
+  CB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace cb

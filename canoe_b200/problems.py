@@ -1,0 +1,201 @@
+"""Seeded synthetic initial states (problem generators) of the configurations.
+
+C1  2-D dry rising thermal bubble, restated from the reference's
+    MeshBlock::ProblemGenerator of examples/2019-Li-snap/robert.cpp:72-114
+    (Gaussian bubble: a = 0, s = radius).
+C2  3-D moist convection: dry adiabat capped by an isothermal layer, H2O at
+    80 % relative humidity, liquid and ice at zero, seeded temperature noise
+    near the ground (the moist-adiabat setup of src/snap/
+    setup_moist_adiabatic_profile.cpp:7-90 restated for a dry adiabat).
+C5  batched uneven blocks: C2's column physics on blocks of seeded sizes.
+
+Every generator returns a :class:`Problem`: the block configuration (a
+ctypes BlockConfig) and the conserved state u laid out (NV, nc3, nc2, nc1)
+with zeroed ghost cells.
+"""
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import thermo as T
+from ._abi import (BC_PERIODIC, BC_REFLECT, FP64, NGHOST, RECON_PLM, RECON_PPM,
+                   RS_HLLC, RS_LMARS, BlockConfig)
+
+
+@dataclass
+class Problem:
+    name: str
+    cfg: BlockConfig
+    x1f: np.ndarray
+    u: np.ndarray
+    w: np.ndarray
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def ny(self):
+        return self.cfg.thermo.ny
+
+    @property
+    def nv(self):
+        return 5 + self.cfg.thermo.ny
+
+    def interior(self, a):
+        ng = NGHOST
+        nx1, nx2, nx3 = self.cfg.nx1, self.cfg.nx2, self.cfg.nx3
+        ks = ng if nx3 > 1 else 0
+        js = ng if nx2 > 1 else 0
+        return a[..., ks:ks + nx3, js:js + nx2, ng:ng + nx1]
+
+
+def make_config(nx1, nx2, nx3, x1f, dx2, dx3, th, bc, recon, rsolver,
+                implicit_flag=0, satadj=0, cfl=0.8, precision=FP64):
+    cfg = BlockConfig()
+    cfg.nx1, cfg.nx2, cfg.nx3 = nx1, nx2, nx3
+    for q in range(6):
+        cfg.bc[q] = bc[q]
+    cfg.x2min = 0.0
+    cfg.x3min = 0.0
+    cfg.dx2, cfg.dx3 = dx2, dx3
+    x1f = np.ascontiguousarray(x1f, dtype=np.float64)
+    cfg.h_x1f = x1f.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    cfg.recon, cfg.rsolver = recon, rsolver
+    cfg.implicit_flag, cfg.precision, cfg.satadj = implicit_flag, precision, satadj
+    cfg.cfl = cfl
+    cfg.thermo = th
+    return cfg, x1f
+
+
+def _shape(nx1, nx2, nx3, nv):
+    nc1 = nx1 + 2 * NGHOST
+    nc2 = nx2 + 2 * NGHOST if nx2 > 1 else 1
+    nc3 = nx3 + 2 * NGHOST if nx3 > 1 else 1
+    return (nv, nc3, nc2, nc1)
+
+
+def _embed(prob_shape, w_int, nx1, nx2, nx3):
+    w = np.zeros(prob_shape)
+    ks = NGHOST if nx3 > 1 else 0
+    js = NGHOST if nx2 > 1 else 0
+    w[:, ks:ks + nx3, js:js + nx2, NGHOST:NGHOST + nx1] = w_int
+    return w
+
+
+def bubble2d(nx1=150, nx2=100, x1max=1500.0, x2max=1000.0, dT=0.5, xc=500.0,
+             zc=260.0, s=250.0, a=0.0, Ts=300.0, p0=1.0e5, grav=9.81,
+             gamma=1.4, cfl=0.8, recon=RECON_PLM, rsolver=RS_LMARS):
+    """C1: robert.cpp:72-114 with x1 vertical, nx3 = 1, reflecting walls."""
+    th = T.dry(gammad=gamma, grav=-grav)
+    Rd = th.rd
+    cp = gamma / (gamma - 1.0) * Rd
+    x1f = np.linspace(0.0, x1max, nx1 + 1)
+    x1v = 0.5 * (x1f[1:] + x1f[:-1])
+    dx2 = x2max / nx2
+    x2v = (np.arange(nx2) + 0.5) * dx2
+    z, x = np.meshgrid(x1v, x2v, indexing="ij")  # (nx1, nx2)
+    r = np.sqrt((x - xc) ** 2 + (z - zc) ** 2)
+    temp = Ts - grav * z / cp
+    pres = p0 * (temp / Ts) ** (cp / Rd)
+    bub = np.where(r <= a, dT, dT * np.exp(-((r - a) ** 2) / (s * s)))
+    temp = temp + bub * (pres / p0) ** (Rd / cp)
+    rho = pres / (Rd * temp)
+    nv = 5
+    w_int = np.zeros((nv, 1, nx2, nx1))
+    w_int[0, 0] = rho.T
+    w_int[4, 0] = pres.T
+    shape = _shape(nx1, nx2, 1, nv)
+    w = _embed(shape, w_int, nx1, nx2, 1)
+    u = T.prim_to_cons(th, w)
+    u[:, :, :, :NGHOST] = 0.0
+    u[:, :, :, NGHOST + nx1:] = 0.0
+    u = _embed(shape, u[:, 0:1, NGHOST:NGHOST + nx2, NGHOST:NGHOST + nx1], nx1, nx2, 1)
+    bc = [BC_REFLECT] * 4 + [BC_PERIODIC] * 2
+    cfg, x1f = make_config(nx1, nx2, 1, x1f, dx2, 1.0, th, bc, recon, rsolver,
+                           implicit_flag=0, satadj=0, cfl=cfl)
+    return Problem("C1-bubble2d", cfg, x1f, u, w, dict(dt_hint=None))
+
+
+def moist_profile(th, z, Ts=300.0, Ttop=200.0, ps=1.0e5, rh=0.8, zmoist=10.0e3,
+                  nsub=16):
+    """Horizontally uniform moist column at heights z (cell centres):
+    T = max(Ts - g z / cp_d, Ttop); H2O at `rh` of saturation below zmoist and
+    at min(q(zmoist), rh q_sat) above; hydrostatic pressure integrated in
+    log p with the gas constant of the moist mixture.  Returns T, p, q_v."""
+    g = -th.grav
+    cpd = th.rd * th.gammad / (th.gammad - 1.0)
+    gam = g / cpd
+    imr = th.inv_mu_ratio_m1[0] if th.nvapor else 0.0
+    rv = th.rd * (1.0 + imr)
+
+    def temp(zz):
+        return np.maximum(Ts - gam * zz, Ttop)
+
+    def qv_rh(tt, pp):
+        if not th.nvapor:
+            return 0.0 * tt
+        e = rh * T.svp(th, 0, tt)
+        e = np.minimum(e, 0.5 * pp)
+        return (e / rv) / ((pp - e) / th.rd + e / rv)
+
+    # integrate ln p from the ground on a fine grid
+    zs = np.concatenate([[0.0], z])
+    lnp = np.log(ps)
+    p_out = np.empty_like(z)
+    q_out = np.empty_like(z)
+    q10 = None
+    zcur = 0.0
+    for n, zt in enumerate(z):
+        h = (zt - zcur) / nsub
+        for _ in range(nsub):
+            zm = zcur + 0.5 * h
+            tm = temp(zm)
+            pm = np.exp(lnp)
+            qm = qv_rh(tm, pm)
+            if q10 is not None and zm > zmoist:
+                qm = min(qm, q10)
+            rm = th.rd * (1.0 + imr * qm)
+            lnp -= g * h / (rm * tm)
+            zcur += h
+        p_out[n] = np.exp(lnp)
+        q = qv_rh(temp(zt), p_out[n])
+        if zt <= zmoist:
+            q10 = q
+        elif q10 is not None:
+            q = min(q, q10)
+        q_out[n] = q
+    return temp(z), p_out, q_out
+
+
+def moist3d(nx1=128, nx2=256, nx3=256, x1max=16.0e3, x2max=64.0e3, x3max=64.0e3,
+            seed=20240601, noise=0.1, noise_depth=1.0e3, implicit_flag=1,
+            recon=RECON_PPM, rsolver=RS_HLLC, satadj=1, cfl=0.8, th=None):
+    """C2: 3-D moist convection LES initial state."""
+    th = th or T.earth_moist()
+    ny = th.ny
+    nv = 5 + ny
+    x1f = np.linspace(0.0, x1max, nx1 + 1)
+    z = 0.5 * (x1f[1:] + x1f[:-1])
+    temp, pres, qv = moist_profile(th, z)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dtn = rng.uniform(-noise, noise, size=(nx3, nx2, nx1))
+    dtn *= (z < noise_depth)[None, None, :]
+    tt = temp[None, None, :] + dtn
+    q = np.zeros((max(ny, 1), nx3, nx2, nx1))
+    if ny:
+        q[0] = qv[None, None, :]
+    feps = T.feps_of(th, q[:ny]) if ny else 1.0
+    pp = np.broadcast_to(pres[None, None, :], tt.shape)
+    rho = pp / (th.rd * feps * tt)
+    w_int = np.zeros((nv, nx3, nx2, nx1))
+    w_int[0] = rho
+    for n in range(1, ny + 1):
+        w_int[n] = q[n - 1]
+    w_int[4 + ny] = pp
+    shape = _shape(nx1, nx2, nx3, nv)
+    u_int = T.prim_to_cons(th, w_int)
+    u = _embed(shape, u_int, nx1, nx2, nx3)
+    w = _embed(shape, w_int, nx1, nx2, nx3)
+    bc = [BC_REFLECT, BC_REFLECT, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC]
+    cfg, x1f = make_config(nx1, nx2, nx3, x1f, x2max / nx2, x3max / nx3, th, bc, recon,
+                           rsolver, implicit_flag=implicit_flag, satadj=satadj, cfl=cfl)
+    return Problem("C2-moist3d", cfg, x1f, u, w, dict(seed=seed))

@@ -1,0 +1,221 @@
+/*
+ * canoe_b200.h -- C ABI of the B200-native dynamical-core hot path of canoe.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns an int status (0 = success, see canoe_status). Arrays follow the
+ * reference layout AthenaArray<Real>(NV, nc3, nc2, nc1) with i (x1, the
+ * vertical) fastest and NGHOST = 3 ghost cells on each side of every active
+ * dimension (canoe src/interface/hydro.hpp:54-67).  Variable slots are
+ * IDN = 0 (dry density in the conserved state, total density in the
+ * primitive state), 1..ny mass fractions (primitive) or species densities
+ * (conserved), IVX = 1+ny, IVY, IVZ, IPR = IEN = 4+ny
+ * (canoe src/tasklist/implicit_hydro_tasks.cpp:300-311).
+ *
+ * Pointers named d_* are device pointers (cudaMalloc'd by the caller),
+ * h_* are host pointers.  `stream` is a cudaStream_t passed as void*.
+ *
+ * Each declaration names the reference interface it replaces (file:line,
+ * relative to the canoe source tree; Athena++ functions are those hooked by
+ * canoe's patches).
+ */
+#ifndef CANOE_B200_H_
+#define CANOE_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CANOE_NGHOST 3
+#define CANOE_MAX_NY 8    /* max mass-fraction slots (vapors + clouds) */
+#define CANOE_MAX_VAPOR 4 /* max condensable vapors                    */
+#define CANOE_MAX_NV (5 + CANOE_MAX_NY)
+
+/* status codes */
+enum canoe_status {
+  CANOE_OK = 0,
+  CANOE_ERR_ARG = 1,      /* invalid argument (size, null pointer, flag)   */
+  CANOE_ERR_CUDA = 2,     /* a CUDA runtime call failed                    */
+  CANOE_ERR_NUMERIC = 3,  /* device error word set (NaN / negative p, rho) */
+  CANOE_ERR_NOCONV = 4,   /* Newton iteration did not converge             */
+  CANOE_ERR_UNSUPPORTED = 5
+};
+
+/* device error-word bits (canoe src/checks.cpp:53-149 glog checks) */
+enum canoe_errbit {
+  CANOE_EBIT_NEG_DENSITY = 1,
+  CANOE_EBIT_NEG_PRESSURE = 2,
+  CANOE_EBIT_NAN = 4,
+  CANOE_EBIT_SATADJ_NOCONV = 8,
+  CANOE_EBIT_SATADJ_FALLBACK = 16
+};
+
+/* boundary flags (Athena BoundaryFlag subset used on this path) */
+enum canoe_bc { CANOE_BC_REFLECT = 0, CANOE_BC_PERIODIC = 1, CANOE_BC_OUTFLOW = 2 };
+
+/* reconstruction order (Athena `xorder`): 2 = PLM, 3 = PPM */
+enum canoe_recon { CANOE_RECON_PLM = 2, CANOE_RECON_PPM = 3 };
+
+/* Riemann solver (canoe RSOLVER, src/snap/CMakeLists.txt:28) */
+enum canoe_rsolver { CANOE_RSOLVER_LMARS = 0, CANOE_RSOLVER_HLLC = 1 };
+
+/* precision of reconstruction + Riemann fluxes */
+enum canoe_precision { CANOE_FP64 = 0, CANOE_FP32_PERTURBATION = 1 };
+
+/*
+ * Ideal-moist thermodynamics (snapy IdealMoist + kintera ThermoY parameters).
+ * Slot n = 1..ny is stored at index n-1 of the per-slot arrays, matching
+ * `cv_ratio_m1[n - 1]` / `inv_mu_ratio_m1[n - 1]` in
+ * canoe src/interface/eos.hpp:48-67.  Vapors occupy slots 1..nvapor, clouds
+ * nvapor+1..ny.
+ */
+typedef struct canoe_thermo {
+  int32_t ny;      /* vapors + clouds                                   */
+  int32_t nvapor;  /* vapors (slots 1..nvapor)                          */
+  double rd;       /* dry specific gas constant [J/kg/K]   eos.hpp:14   */
+  double gammad;   /* dry adiabatic index                  eos.hpp:18   */
+  double grav;     /* signed x1 gravity (hsrc.GetG1()), <0 points to -x1 */
+  double cv_ratio_m1[CANOE_MAX_NY];     /* cv_n / cv_d - 1                 */
+  double inv_mu_ratio_m1[CANOE_MAX_NY]; /* mu_d / mu_n - 1 (vapors)        */
+  double u0[CANOE_MAX_NY];              /* latent energy offset [J/kg]     */
+  /* phase change, per vapor v = 0..nvapor-1 (kintera "ideal" nucleation) */
+  int32_t liq_slot[CANOE_MAX_VAPOR];    /* slot of the liquid, -1 if none  */
+  int32_t ice_slot[CANOE_MAX_VAPOR];    /* slot of the ice, -1 if none     */
+  double t3[CANOE_MAX_VAPOR];           /* triple-point temperature [K]    */
+  double p3[CANOE_MAX_VAPOR];           /* triple-point pressure [Pa]      */
+  double beta_l[CANOE_MAX_VAPOR], delta_l[CANOE_MAX_VAPOR];
+  double beta_s[CANOE_MAX_VAPOR], delta_s[CANOE_MAX_VAPOR];
+} canoe_thermo_t;
+
+/* Newton saturation-adjustment controls */
+typedef struct canoe_satadj_opts {
+  double tol;      /* |dT| stopping tolerance [K]                       */
+  int32_t max_iter;/* Newton iterations before the bracketing fallback  */
+  int32_t warm;    /* 1: take the initial guess from t_guess[]          */
+} canoe_satadj_opts_t;
+
+/* One MeshBlock: a Cartesian (or cubed-sphere panel) block. */
+typedef struct canoe_block_config {
+  int32_t nx1, nx2, nx3;  /* interior cells; nx3 == 1 => 2-D (no x3 ghosts) */
+  int32_t bc[6];          /* ix1, ox1, ix2, ox2, ix3, ox3 (canoe_bc)          */
+  double x2min, x3min;    /* lower edges                                      */
+  double dx2, dx3;        /* uniform widths                                   */
+  const double *h_x1f;    /* nx1+1 interior x1 face positions (nonuniform ok) */
+  int32_t recon;          /* canoe_recon                                      */
+  int32_t rsolver;        /* canoe_rsolver                                    */
+  int32_t implicit_flag;  /* bit0 X1, bit3 full 5x5 (implicit_solver.cpp:47)  */
+  int32_t precision;      /* canoe_precision                                  */
+  int32_t satadj;         /* 1: saturation adjustment at the last RK stage    */
+  double cfl;             /* CFL number for canoe_block_new_dt                */
+  canoe_thermo_t thermo;
+} canoe_block_config_t;
+
+typedef struct canoe_block *canoe_block_t;
+
+/* ---------------- version / diagnostics ---------------- */
+const char *canoe_version(void);
+const char *canoe_last_error(void);
+int canoe_device_sm_count(int *out);
+
+/* ---------------- operator-level entry points (device pointers) --------- */
+
+/* Hydro::RiemannSolver, LMARS: canoe src/snap/riemann/lmars.cpp:19-85.
+ * d_wl, d_wr: (NV, n) face states; d_flx: (NV, n) fluxes.  ivx is the
+ * variable slot of the normal velocity (IVX, IVY or IVZ). */
+int canoe_riemann_lmars(const canoe_thermo_t *th, int ivx, const double *d_wl,
+                        const double *d_wr, double *d_flx, int64_t n,
+                        void *stream);
+
+/* Hydro::RiemannSolver, HLLC: canoe src/snap/riemann/hllc_transform.cpp:25-233
+ * (Cartesian branch). Same layout as canoe_riemann_lmars. */
+int canoe_riemann_hllc(const canoe_thermo_t *th, int ivx, const double *d_wl,
+                       const double *d_wr, double *d_flx, int64_t n,
+                       void *stream);
+
+/* Saturation adjustment, kintera ThermoY::forward(rho, intEng, yfrac) as
+ * called from ImplicitHydroTasks::UpdateAllConserved,
+ * canoe src/tasklist/implicit_hydro_tasks.cpp:290-313.  Operates in place on
+ * conserved cells d_u laid out (NV, ncells); d_t_guess (ncells, may be NULL
+ * unless opts->warm) is the initial temperature; d_t_out (may be NULL)
+ * receives the converged temperature; d_iters (may be NULL) the Newton
+ * iteration count per cell.  d_stats[0..3] (may be NULL) accumulates
+ * {cells, total iterations, fallbacks, non-converged}. */
+int canoe_saturation_adjust(const canoe_thermo_t *th,
+                            const canoe_satadj_opts_t *opts, double *d_u,
+                            int64_t ncells, const double *d_t_guess,
+                            double *d_t_out, int32_t *d_iters,
+                            unsigned long long *d_stats, void *stream);
+
+/* ---------------- MeshBlock-level entry points ---------------- */
+
+/* MeshBlock + MeshBlock::Impl construction (canoe src/mesh_setup.cpp:98-101,
+ * src/impl.cpp:38-112): allocates every device array of the block. */
+int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out);
+int canoe_block_destroy(canoe_block_t b);
+/* sizes: nv, nc1, nc2, nc3 (with ghosts) */
+int canoe_block_dims(canoe_block_t b, int32_t *nv, int32_t *nc1, int32_t *nc2,
+                     int32_t *nc3);
+
+/* upload / download the conserved state u and primitive state w
+ * (NV, nc3, nc2, nc1) host arrays; set_conserved recomputes w (cons->prim +
+ * boundary ghosts).  Blocking. */
+int canoe_block_set_conserved(canoe_block_t b, const double *h_u);
+int canoe_block_get_conserved(canoe_block_t b, double *h_u);
+int canoe_block_get_primitive(canoe_block_t b, double *h_w);
+/* device views of the live state (for zero-copy callers) */
+int canoe_block_device_ptrs(canoe_block_t b, double **d_u, double **d_w);
+int canoe_block_set_stream(canoe_block_t b, void *stream);
+
+/* Hydro::CalculateFluxes(w, b, bcc, order): Athena calculate_fluxes.cpp with
+ * canoe patches/19.calculate_fluxes.patch:19-185 (ChangeToTemperature at
+ * :24, RestoreFromTemperature at :42, RiemannSolver per direction).  Writes
+ * the three face-flux arrays: d_flx1 (NV, nc3, nc2, nc1+1), d_flx2
+ * (NV, nc3, nc2+1, nc1), d_flx3 (NV, nc3+1, nc2, nc1); interior faces only. */
+int canoe_block_calculate_fluxes(canoe_block_t b, double *d_flx1,
+                                 double *d_flx2, double *d_flx3);
+
+/* ImplicitSolver::SolveImplicit3D(du, w, dt), X1 direction:
+ * canoe src/snap/implicit/solve_implicit_3d.cpp:91-142 with
+ * PartialCorrection (partial_correction.cpp:26-170) or FullCorrection
+ * (full_correction.cpp:32-161) and ForwardSweep / BackwardSubstitution
+ * (forward_backward.hpp:15-137).  d_du (NV, nc3, nc2, nc1) is corrected in
+ * place; the block's current primitive state is used as w. */
+int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt);
+
+/* One full time step of the block (all RK3 stages): the Athena task list as
+ * rewritten by ImplicitHydroTasks (src/tasklist/implicit_hydro_tasks.cpp:
+ * 45-313): CalculateFluxes -> IntegrateHydro -> AddSourceTerms ->
+ * ImplicitCorrection -> UpdateAllConserved -> boundaries -> cons2prim.
+ * dt < 0 uses the block's own CFL time step (Hydro::NewBlockTimeStep with
+ * patches/21.new_blockdt.patch) computed on the device. */
+int canoe_block_step(canoe_block_t b, double dt);
+
+/* Capture one step (all RK stages, device dt) as a CUDA graph on first use and
+ * replay it for every canoe_block_step(b, dt <= 0) call.  No reference
+ * counterpart: the reference drives the task list from the host per stage
+ * (main.cpp:119-121). */
+int canoe_block_use_graph(canoe_block_t b, int on);
+
+/* One step like canoe_block_step, timing each kernel class with CUDA events
+ * on the block's stream; adds milliseconds to ms[0..6] = {x1 flux, x2 flux,
+ * x3 flux, RK update + implicit solve, saturation adjustment, cons->prim +
+ * ghosts, dt}.  No reference counterpart (the reference times whole runs,
+ * src/mesh_destroy.cpp:43-53). */
+int canoe_block_step_profile(canoe_block_t b, double dt, float *ms, int nclass);
+
+/* wait for the block's stream (steps are asynchronous) */
+int canoe_block_synchronize(canoe_block_t b);
+
+/* Hydro::NewBlockTimeStep with canoe patches/21.new_blockdt.patch:20-40;
+ * reads back the CFL time step of the current state. */
+int canoe_block_new_dt(canoe_block_t b, double *dt_out);
+
+/* read and clear the block's device error word (canoe_errbit bits) */
+int canoe_block_error_word(canoe_block_t b, uint32_t *bits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CANOE_B200_H_ */

@@ -1,0 +1,186 @@
+// capi.cpp -- C entry points of the oracle for the Python test harness
+// (ctypes).  TEST INFRASTRUCTURE ONLY.
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "oracle.hpp"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+using oracle::Block;
+
+static thread_local std::string g_err;
+
+extern "C" {
+
+const char *oracle_last_error() { return g_err.c_str(); }
+
+int oracle_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+void *oracle_block_new(const canoe_block_config_t *cfg) {
+  try {
+    Block *b = new Block();
+    oracle::block_init(*b, *cfg);
+    return b;
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+
+void oracle_block_free(void *h) { delete static_cast<Block *>(h); }
+
+void oracle_block_set_roundtrip(void *h, int on) {
+  static_cast<Block *>(h)->fix_roundtrip = on != 0;
+}
+
+int oracle_block_set_conserved(void *h, const double *u) {
+  Block &b = *static_cast<Block *>(h);
+  std::memcpy(b.u.data(), u, b.u.size() * sizeof(double));
+  oracle::cons_to_prim_block(b);
+  return 0;
+}
+
+int oracle_block_set_primitive(void *h, const double *w) {
+  Block &b = *static_cast<Block *>(h);
+  std::memcpy(b.w.data(), w, b.w.size() * sizeof(double));
+  return 0;
+}
+
+int oracle_block_get_conserved(void *h, double *u) {
+  Block &b = *static_cast<Block *>(h);
+  std::memcpy(u, b.u.data(), b.u.size() * sizeof(double));
+  return 0;
+}
+
+int oracle_block_get_primitive(void *h, double *w) {
+  Block &b = *static_cast<Block *>(h);
+  std::memcpy(w, b.w.data(), b.w.size() * sizeof(double));
+  return 0;
+}
+
+int oracle_block_calculate_fluxes(void *h, double *f1, double *f2, double *f3) {
+  Block &b = *static_cast<Block *>(h);
+  try {
+    std::fill(b.flx1.begin(), b.flx1.end(), 0.);
+    std::fill(b.flx2.begin(), b.flx2.end(), 0.);
+    std::fill(b.flx3.begin(), b.flx3.end(), 0.);
+    oracle::calculate_fluxes(b);
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  if (f1) std::memcpy(f1, b.flx1.data(), b.flx1.size() * sizeof(double));
+  if (f2) std::memcpy(f2, b.flx2.data(), b.flx2.size() * sizeof(double));
+  if (f3) std::memcpy(f3, b.flx3.data(), b.flx3.size() * sizeof(double));
+  return 0;
+}
+
+int oracle_block_solve_implicit(void *h, double *du, double dt) {
+  Block &b = *static_cast<Block *>(h);
+  try {
+    std::vector<double> d(du, du + b.u.size());
+    oracle::solve_implicit(b, d, dt);
+    std::memcpy(du, d.data(), d.size() * sizeof(double));
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  return 0;
+}
+
+int oracle_block_step(void *h, double dt, int nsteps) {
+  Block &b = *static_cast<Block *>(h);
+  try {
+    for (int s = 0; s < nsteps; ++s) {
+      double d = dt > 0. ? dt : oracle::new_dt(b);
+      oracle::step(b, d);
+    }
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  return 0;
+}
+
+double oracle_block_new_dt(void *h) { return oracle::new_dt(*static_cast<Block *>(h)); }
+
+int oracle_riemann(int rsolver, const canoe_thermo_t *th, int ivx,
+                   const double *wl, const double *wr, double *flx, int64_t n) {
+  if (rsolver == CANOE_RSOLVER_LMARS)
+    oracle::riemann_lmars(*th, ivx, wl, wr, flx, n);
+  else
+    oracle::riemann_hllc(*th, ivx, wl, wr, flx, n);
+  return 0;
+}
+
+int oracle_cons_to_prim(const canoe_thermo_t *th, const double *u, double *w,
+                        int64_t n) {
+  for (int64_t c = 0; c < n; ++c) oracle::cons_to_prim_cell(*th, u + c, w + c, n);
+  return 0;
+}
+
+int oracle_prim_to_cons(const canoe_thermo_t *th, const double *w, double *u,
+                        int64_t n) {
+  for (int64_t c = 0; c < n; ++c) oracle::prim_to_cons_cell(*th, w + c, u + c, n);
+  return 0;
+}
+
+int oracle_satadj(const canoe_thermo_t *th, const canoe_satadj_opts_t *o,
+                  double *u, int64_t n, const double *t_guess, double *t_out,
+                  int32_t *iters, int32_t *flags) {
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    oracle::SatResult r =
+        oracle::satadj_cell(*th, *o, u + c, n, t_guess ? t_guess[c] : 0.);
+    if (t_out) t_out[c] = r.t;
+    if (iters) iters[c] = r.iters;
+    if (flags) flags[c] = (r.fallback ? 1 : 0) | (r.converged ? 0 : 2);
+  }
+  return 0;
+}
+
+// params: w1[nh*4], b1[nh], w2[nh*nh], b2[nh], w3[nh], b3[1], contiguous
+static oracle::Mlp unpack(const double *p, int nh) {
+  oracle::Mlp m;
+  m.nh = nh;
+  const double *q = p;
+  m.w1.assign(q, q + nh * 4); q += nh * 4;
+  m.b1.assign(q, q + nh); q += nh;
+  m.w2.assign(q, q + nh * nh); q += nh * nh;
+  m.b2.assign(q, q + nh); q += nh;
+  m.w3.assign(q, q + nh); q += nh;
+  m.b3.assign(q, q + 1);
+  return m;
+}
+
+int oracle_mlp_forward(const double *params, int nh, const double *x, int64_t n,
+                       double *y) {
+  oracle::mlp_forward(unpack(params, nh), x, n, y);
+  return 0;
+}
+
+double oracle_mlp_loss_grad(const double *params, int nh, const double *x,
+                            const double *y, int64_t n, double *grad) {
+  oracle::Mlp m = unpack(params, nh), g;
+  double loss = oracle::mlp_loss_grad(m, x, y, n, g);
+  double *q = grad;
+  for (auto *v : {&g.w1, &g.b1, &g.w2, &g.b2, &g.w3, &g.b3}) {
+    std::memcpy(q, v->data(), v->size() * sizeof(double));
+    q += v->size();
+  }
+  return loss;
+}
+
+}  // extern "C"

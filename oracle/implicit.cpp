@@ -1,0 +1,330 @@
+// implicit.cpp -- oracle restatement of canoe's implicit vertical solver,
+// X1 direction: ImplicitSolver::SolveImplicit3D (src/snap/implicit/
+// solve_implicit_3d.cpp:91-142) -> PartialCorrection (partial_correction.cpp:
+// 26-170) / FullCorrection (full_correction.cpp:32-161) -> ForwardSweep /
+// BackwardSubstitution (forward_backward.hpp:15-137), single block per
+// column (first_block = last_block = true, no MPI pipeline), non-periodic x1.
+// Small dense matrices are plain arrays instead of Eigen; 3x3 inverses use
+// the adjugate, 5x5 inverses Gauss-Jordan with partial pivoting.
+// TEST INFRASTRUCTURE ONLY.
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "oracle.hpp"
+
+namespace oracle {
+
+namespace {
+
+template <int N>
+struct Mat {
+  double a[N][N];
+  void zero() { std::memset(a, 0, sizeof(a)); }
+};
+template <int N>
+struct Vec {
+  double a[N];
+};
+
+template <int N>
+Mat<N> mul(const Mat<N> &x, const Mat<N> &y) {
+  Mat<N> r;
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      double s = 0.;
+      for (int k = 0; k < N; ++k) s += x.a[i][k] * y.a[k][j];
+      r.a[i][j] = s;
+    }
+  return r;
+}
+template <int N>
+Vec<N> mul(const Mat<N> &x, const Vec<N> &y) {
+  Vec<N> r;
+  for (int i = 0; i < N; ++i) {
+    double s = 0.;
+    for (int k = 0; k < N; ++k) s += x.a[i][k] * y.a[k];
+    r.a[i] = s;
+  }
+  return r;
+}
+
+Mat<3> inverse(const Mat<3> &m) {
+  const double(*a)[3] = m.a;
+  double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+  double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+  double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+  double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+  double id = 1. / det;
+  Mat<3> r;
+  r.a[0][0] = c00 * id;
+  r.a[1][0] = c01 * id;
+  r.a[2][0] = c02 * id;
+  r.a[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id;
+  r.a[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id;
+  r.a[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id;
+  r.a[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id;
+  r.a[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id;
+  r.a[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id;
+  return r;
+}
+
+Mat<5> inverse(const Mat<5> &m) {
+  double a[5][10];
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) {
+      a[i][j] = m.a[i][j];
+      a[i][5 + j] = (i == j) ? 1. : 0.;
+    }
+  for (int c = 0; c < 5; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 5; ++r)
+      if (std::fabs(a[r][c]) > std::fabs(a[p][c])) p = r;
+    if (p != c)
+      for (int j = 0; j < 10; ++j) std::swap(a[c][j], a[p][j]);
+    double ip = 1. / a[c][c];
+    for (int j = 0; j < 10; ++j) a[c][j] *= ip;
+    for (int r = 0; r < 5; ++r) {
+      if (r == c) continue;
+      double f = a[r][c];
+      if (f != 0.)
+        for (int j = 0; j < 10; ++j) a[r][j] -= f * a[c][j];
+    }
+  }
+  Mat<5> r;
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) r.a[i][j] = a[i][5 + j];
+  return r;
+}
+
+// FluxJacobian, flux_decomposition.hpp:102-120 (X1: v1 = w[IVX]).
+void flux_jacobian(Mat<5> &d, double gm1, const double *w, int IVX, int IPR) {
+  double v1 = w[IVX], v2 = w[IVX + 1], v3 = w[IVX + 2];
+  double rho = w[0], pres = w[IPR];
+  double s2 = v1 * v1 + v2 * v2 + v3 * v3;
+  double c1 = ((gm1 - 1) * s2 / 2 - (gm1 + 1) / gm1 * pres / rho) * v1;
+  double c2 = (gm1 + 1) / gm1 * pres / rho + s2 / 2 - gm1 * v1 * v1;
+  double r[25] = {0,     1.,           0.,         0.,         0.,
+                  gm1 * s2 / 2 - v1 * v1, (2. - gm1) * v1, -gm1 * v2, -gm1 * v3, gm1,
+                  -v1 * v2, v2,        v1,         0.,         0.,
+                  -v1 * v3, v3,        0.,         v1,         0.,
+                  c1,    c2,           -gm1 * v2 * v1, -gm1 * v3 * v1, (gm1 + 1) * v1};
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) d.a[i][j] = r[i * 5 + j];
+}
+
+// RoeAverage, flux_decomposition.hpp:34-67
+void roe_average(double *prim, double gm1, const double *wl, const double *wr,
+                 int ny) {
+  int IVX = 1 + ny, IVY = 2 + ny, IVZ = 3 + ny, IPR = 4 + ny;
+  double sqrtdl = std::sqrt(wl[0]);
+  double sqrtdr = std::sqrt(wr[0]);
+  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  prim[0] = sqrtdl * sqrtdr;
+  prim[IVX] = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
+  prim[IVY] = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
+  prim[IVZ] = (sqrtdl * wl[IVZ] + sqrtdr * wr[IVZ]) * isdlpdr;
+  for (int i = 1; i < IVX; ++i) prim[i] = (sqrtdl * wl[i] + sqrtdr * wr[i]) * isdlpdr;
+  double el = wl[IPR] / gm1 +
+              0.5 * wl[0] * (wl[IVX] * wl[IVX] + wl[IVY] * wl[IVY] + wl[IVZ] * wl[IVZ]);
+  double er = wr[IPR] / gm1 +
+              0.5 * wr[0] * (wr[IVX] * wr[IVX] + wr[IVY] * wr[IVY] + wr[IVZ] * wr[IVZ]);
+  double hbar = ((el + wl[IPR]) / sqrtdl + (er + wr[IPR]) / sqrtdr) * isdlpdr;
+  prim[IPR] = (hbar - 0.5 * (prim[IVX] * prim[IVX] + prim[IVY] * prim[IVY] +
+                             prim[IVZ] * prim[IVZ])) *
+              gm1 / (gm1 + 1.) * prim[0];
+}
+
+// |A| = R |Lambda| R^-1: Eigenvalue (:70-75) and Eigenvector (:78-99)
+void abs_jacobian(Mat<5> &A, const double *prim, double cs, double gm1, int ny) {
+  int IVX = 1 + ny, IPR = 4 + ny;
+  double r = prim[0], u = prim[IVX], v = prim[IVX + 1], w = prim[IVX + 2],
+         p = prim[IPR];
+  double ke = 0.5 * (u * u + v * v + w * w);
+  double hp = (gm1 + 1.) / gm1 * p / r;
+  double h = hp + ke;
+  double R[25] = {1.,         1., 1.,         0., 0.,  //
+                  u - cs,     u,  u + cs,     0., 0.,  //
+                  v,          v,  v,          1., 0.,  //
+                  w,          w,  w,          0., 1.,  //
+                  h - u * cs, ke, h + u * cs, v,  w};
+  double Ri[25] = {(cs * ke + u * hp) / (2. * cs * hp), (-hp - cs * u) / (2. * cs * hp),
+                   -v / (2. * hp), -w / (2. * hp), 1. / (2. * hp),
+                   (hp - ke) / hp, u / hp, v / hp, w / hp, -1. / hp,
+                   (cs * ke - u * hp) / (2. * cs * hp), (hp - cs * u) / (2. * cs * hp),
+                   -v / (2. * hp), -w / (2. * hp), 1. / (2. * hp),
+                   -v, 0., 1., 0., 0.,
+                   -w, 0., 0., 1., 0.};
+  double lam[5] = {std::fabs(u - cs), std::fabs(u), std::fabs(u + cs), std::fabs(u),
+                   std::fabs(u)};
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) {
+      double s = 0.;
+      for (int k = 0; k < 5; ++k) s += (R[i * 5 + k] * lam[k]) * Ri[k * 5 + j];
+      A.a[i][j] = s;
+    }
+}
+
+template <int N>
+Mat<N> reduce(const Mat<5> &m) {
+  Mat<N> r;
+  if constexpr (N == 5) {
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j) r.a[i][j] = m.a[i][j];
+  } else {
+    static const int sel[3] = {0, 1, 4};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) r.a[i][j] = m.a[sel[i]][sel[j]];
+  }
+  return r;
+}
+
+template <int N>
+void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
+  const int nc1 = b.nc1, nv = b.nv, ny = b.ny, IVX = b.ivx, IPR = b.ipr;
+  const int is = b.is, ie = b.ie;
+  const size_t s = b.cells();
+  auto W = [&](int i, double *out) {
+    for (int n = 0; n < nv; ++n) out[n] = b.w[b.idx(0, k, j, i) + n * s];
+  };
+  const double gm1 = b.th.gammad - 1.;
+  const double grav = b.th.grav;
+  std::vector<Mat<N>> a(nc1), bb(nc1), c(nc1), dfdq(nc1);
+  std::vector<Vec<N>> delta(nc1);
+  Mat<5> full;
+  double wl[CANOE_MAX_NV], wr[CANOE_MAX_NV], prim[CANOE_MAX_NV];
+  // flux Jacobians of cells is-2..ie+1 (partial_correction.cpp:90-101)
+  for (int i = is - 2; i <= ie + 1; ++i) {
+    W(i, wr);
+    flux_jacobian(full, gm1, wr, IVX, IPR);
+    dfdq[i] = reduce<N>(full);
+  }
+  Mat<N> Phi, Dt, Bnd;
+  Phi.zero();
+  Dt.zero();
+  Bnd.zero();
+  for (int d = 0; d < N; ++d) {
+    Dt.a[d][d] = 1. / dt;
+    Bnd.a[d][d] = 1.;
+  }
+  Bnd.a[1][1] = -1.;
+  if constexpr (N == 3) {  // partial_correction.cpp:59-61 (row-major comma fill)
+    Phi.a[1][0] = grav;
+    Phi.a[2][1] = grav;
+  } else {  // full_correction.cpp:57-61
+    Phi.a[1][0] = grav;
+    Phi.a[4][1] = grav;
+  }
+  // left edge |A| at face is-1-1/2 (partial_correction.cpp:103-115)
+  W(is - 2, wl);
+  W(is - 1, wr);
+  roe_average(prim, gm1, wl, wr, ny);
+  double cs = sound_speed(b.th, prim);
+  abs_jacobian(full, prim, cs, gm1, ny);
+  Mat<N> Am = reduce<N>(full), Ap;
+  const double area = b.dx2 * b.dx3;
+  for (int i = is - 1; i <= ie; ++i) {
+    W(i, wl);
+    W(i + 1, wr);
+    roe_average(prim, gm1, wl, wr, ny);
+    cs = sound_speed(b.th, prim);
+    abs_jacobian(full, prim, cs, gm1, ny);
+    Ap = reduce<N>(full);
+    double aleft = area, aright = area, vol = b.dx1f[i] * b.dx2 * b.dx3;
+    for (int r = 0; r < N; ++r)
+      for (int q = 0; q < N; ++q) {
+        a[i].a[r][q] = (Am.a[r][q] * aleft + Ap.a[r][q] * aright +
+                        (aright - aleft) * dfdq[i].a[r][q]) /
+                           (2. * vol) +
+                       Dt.a[r][q] - Phi.a[r][q];
+        bb[i].a[r][q] = -(Am.a[r][q] + dfdq[i - 1].a[r][q]) * aleft / (2. * vol);
+        c[i].a[r][q] = -(Ap.a[r][q] - dfdq[i + 1].a[r][q]) * aright / (2. * vol);
+      }
+    Am = Ap;
+  }
+  // reflecting ends (partial_correction.cpp:153-154)
+  {
+    Mat<N> t = mul(bb[is], Bnd);
+    for (int r = 0; r < N; ++r)
+      for (int q = 0; q < N; ++q) a[is].a[r][q] += t.a[r][q];
+    t = mul(c[ie], Bnd);
+    for (int r = 0; r < N; ++r)
+      for (int q = 0; q < N; ++q) a[ie].a[r][q] += t.a[r][q];
+  }
+  // ForwardSweep (forward_backward.hpp:15-85)
+  auto rhs_of = [&](int i) {
+    Vec<N> r;
+    double r0 = du[b.idx(0, k, j, i)];
+    for (int n = 1; n < IVX; ++n) r0 += du[b.idx(n, k, j, i)];
+    r.a[0] = r0 / dt;
+    r.a[1] = du[b.idx(IVX, k, j, i)] / dt;
+    if constexpr (N == 3) {
+      r.a[2] = du[b.idx(IPR, k, j, i)] / dt;
+    } else {
+      r.a[2] = du[b.idx(IVX + 1, k, j, i)] / dt;
+      r.a[3] = du[b.idx(IVX + 2, k, j, i)] / dt;
+      r.a[4] = du[b.idx(IPR, k, j, i)] / dt;
+    }
+    return r;
+  };
+  {
+    Vec<N> rhs = rhs_of(is);
+    a[is] = inverse(a[is]);
+    delta[is] = mul(a[is], rhs);
+    a[is] = mul(a[is], c[is]);
+  }
+  for (int i = is + 1; i <= ie; ++i) {
+    Vec<N> rhs = rhs_of(i);
+    Mat<N> t = mul(bb[i], a[i - 1]);
+    for (int r = 0; r < N; ++r)
+      for (int q = 0; q < N; ++q) t.a[r][q] = a[i].a[r][q] - t.a[r][q];
+    a[i] = inverse(t);
+    Vec<N> bd = mul(bb[i], delta[i - 1]);
+    for (int r = 0; r < N; ++r) bd.a[r] = rhs.a[r] - bd.a[r];
+    delta[i] = mul(a[i], bd);
+    a[i] = mul(a[i], c[i]);
+  }
+  // BackwardSubstitution (forward_backward.hpp:87-137)
+  for (int i = ie - 1; i >= is; --i) {
+    Vec<N> t = mul(a[i], delta[i + 1]);
+    for (int r = 0; r < N; ++r) delta[i].a[r] -= t.a[r];
+  }
+  for (int i = is; i <= ie; ++i) {
+    double dens = du[b.idx(0, k, j, i)];
+    for (int n = 1; n < IVX; ++n) dens += du[b.idx(n, k, j, i)];
+    dens = delta[i].a[0] - dens;
+    du[b.idx(0, k, j, i)] = delta[i].a[0];
+    for (int n = 1; n < IVX; ++n)
+      du[b.idx(n, k, j, i)] += dens * b.w[b.idx(n, k, j, i)];
+    du[b.idx(IVX, k, j, i)] = delta[i].a[1];
+    if constexpr (N == 3) {
+      du[b.idx(IPR, k, j, i)] = delta[i].a[2];
+    } else {
+      du[b.idx(IVX + 1, k, j, i)] = delta[i].a[2];
+      du[b.idx(IVX + 2, k, j, i)] = delta[i].a[3];
+      du[b.idx(IPR, k, j, i)] = delta[i].a[4];
+    }
+    for (int n = 1; n < IVX; ++n) du[b.idx(0, k, j, i)] -= du[b.idx(n, k, j, i)];
+  }
+}
+
+}  // namespace
+
+void solve_implicit(Block &b, std::vector<double> &du, double dt) {
+  int flag = b.cfg.implicit_flag;
+  if (!(flag & 1)) return;
+  if (b.cfg.bc[0] == CANOE_BC_PERIODIC)
+    throw std::runtime_error("periodic x1 implicit solve is not supported");
+  bool full = flag & 8;
+#pragma omp parallel for collapse(2) schedule(dynamic, 16)
+  for (int k = b.ks; k <= b.ke; ++k)
+    for (int j = b.js; j <= b.je; ++j) {
+      if (full)
+        column<5>(b, du, dt, k, j);
+      else
+        column<3>(b, du, dt, k, j);
+    }
+}
+
+}  // namespace oracle

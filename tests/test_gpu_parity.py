@@ -1,0 +1,261 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances: the FP64 GPU path differs from the oracle only by floating-point
+evaluation order (fused multiply-adds, the parallel hydrostatic scan, the
+fused divergence), so pointwise operators agree to ~1e-14 and a full time
+step to <= 1e-11 relative L2 per variable (the FP64 bar of the path).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from canoe_b200 import MeshBlock, problems, thermo
+from canoe_b200._abi import (BC_REFLECT, RECON_PLM, RECON_PPM, RS_HLLC, RS_LMARS,
+                             SatOpts, check, load)
+from conftest import max_var_rel_l2, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-11
+OP_TOL = 1e-12
+
+
+def perturb(p, seed=7, dv=2.0, drho=0.01, dp=0.002):
+    """Seeded perturbation of a problem's primitive state (velocities, density,
+    pressure) so that every flux component is exercised."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = p.interior(p.w).copy()
+    ny = p.ny
+    w[0] *= 1.0 + drho * rng.uniform(-1, 1, w[0].shape)
+    for n in range(1 + ny, 4 + ny):
+        w[n] += dv * rng.uniform(-1, 1, w[n].shape)
+    w[4 + ny] *= 1.0 + dp * rng.uniform(-1, 1, w[0].shape)
+    if p.cfg.nx3 == 1:
+        w[3 + ny] = 0.0
+    u_int = thermo.prim_to_cons(p.cfg.thermo, w)
+    u = np.zeros_like(p.u)
+    p.interior(u)[...] = u_int
+    p.u = u
+    return p
+
+
+def small_c1(**kw):
+    return problems.bubble2d(nx1=40, nx2=24, x1max=400.0, x2max=240.0, **kw)
+
+
+def small_c2(**kw):
+    args = dict(nx1=24, nx2=16, nx3=12, x1max=3000.0, x2max=4000.0, x3max=3000.0)
+    args.update(kw)
+    return problems.moist3d(**args)
+
+
+# ---------------------------------------------------------------------------
+# pointwise Riemann solvers
+
+
+def random_faces(th, n, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ny = th.ny
+    nv = 5 + ny
+
+    def side():
+        w = np.zeros((nv, n))
+        w[0] = rng.uniform(0.2, 1.5, n)
+        for s in range(1, ny + 1):
+            w[s] = rng.uniform(0.0, 0.02, n)
+        for s in range(1 + ny, 4 + ny):
+            w[s] = rng.uniform(-60.0, 60.0, n)
+        w[4 + ny] = rng.uniform(2e4, 1.2e5, n)
+        return w
+
+    return side(), side()
+
+
+@pytest.mark.parametrize("rs", [RS_LMARS, RS_HLLC])
+@pytest.mark.parametrize("ny_kind", ["dry", "moist"])
+@pytest.mark.parametrize("dirn", [0, 1, 2])
+def test_riemann_faces(oracle_mod, rs, ny_kind, dirn):
+    import torch
+    th = thermo.dry() if ny_kind == "dry" else thermo.earth_moist()
+    n = 4099
+    wl, wr = random_faces(th, n, seed=11 + dirn + 3 * rs)
+    ivx = 1 + th.ny + dirn
+    ref = oracle_mod.riemann(rs, th, ivx, wl, wr)
+    dl = torch.from_numpy(wl).cuda()
+    dr = torch.from_numpy(wr).cuda()
+    df = torch.zeros_like(dl)
+    lib = load()
+    fn = lib.canoe_riemann_lmars if rs == RS_LMARS else lib.canoe_riemann_hllc
+    torch.cuda.synchronize()
+    check(fn(ctypes.byref(th), ivx, dl.data_ptr(), dr.data_ptr(), df.data_ptr(), n, None))
+    torch.cuda.synchronize()
+    got = df.cpu().numpy()
+    scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-300
+    assert np.max(np.abs(got - ref) / scale) < 1e-13
+
+
+def test_riemann_rejects_bad_direction():
+    th = thermo.dry()
+    rc = load().canoe_riemann_hllc(ctypes.byref(th), 0, None, None, None, 0, None)
+    assert rc != 0
+
+
+# ---------------------------------------------------------------------------
+# cons -> prim with boundary ghosts, fluxes, implicit solve, satadj
+
+
+CASES = {
+    "c1_plm_lmars": lambda: small_c1(),
+    "c1_ppm_hllc": lambda: small_c1(recon=RECON_PPM, rsolver=RS_HLLC),
+    "c2_ppm_hllc": lambda: small_c2(),
+    "c2_plm_lmars": lambda: small_c2(recon=RECON_PLM, rsolver=RS_LMARS),
+    "c2_full5x5": lambda: small_c2(implicit_flag=9),
+}
+
+
+@pytest.mark.parametrize("case", ["c1_plm_lmars", "c2_ppm_hllc"])
+def test_cons_to_prim_with_ghosts(oracle_mod, case):
+    p = perturb(CASES[case]())
+    gpu = MeshBlock(p)
+    ora = oracle_mod.OracleBlock(p)
+    assert max_var_rel_l2(gpu.primitive(), ora.primitive()) < 1e-14
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_calculate_fluxes(oracle_mod, case):
+    p = perturb(CASES[case]())
+    gpu = MeshBlock(p)
+    ora = oracle_mod.OracleBlock(p)
+    g = gpu.calculate_fluxes()
+    o = ora.calculate_fluxes()
+    for d, (a, b) in enumerate(zip(g, o)):
+        if d == 2 and p.cfg.nx3 == 1:
+            continue
+        err = max_var_rel_l2(a, b)
+        assert err < OP_TOL, f"x{d + 1} flux rel L2 {err}"
+
+
+@pytest.mark.parametrize("case", ["c2_ppm_hllc", "c2_full5x5"])
+def test_solve_implicit(oracle_mod, case):
+    p = perturb(CASES[case]())
+    gpu = MeshBlock(p)
+    ora = oracle_mod.OracleBlock(p)
+    rng = np.random.Generator(np.random.PCG64(3))
+    du = np.zeros(p.u.shape)
+    p.interior(du)[...] = 1e-3 * rng.standard_normal(p.interior(du).shape) * \
+        np.abs(p.interior(p.u)).mean(axis=(1, 2, 3))[:, None, None, None]
+    dt = 0.5
+    a = gpu.solve_implicit(du, dt)
+    b = ora.solve_implicit(du, dt)
+    assert max_var_rel_l2(p.interior(a), p.interior(b)) < 1e-11
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_step_parity(oracle_mod, case):
+    p = perturb(CASES[case](), dv=0.5)
+    gpu = MeshBlock(p)
+    ora = oracle_mod.OracleBlock(p)
+    dt = ora.new_dt()
+    assert abs(gpu.new_dt() - dt) <= 1e-12 * dt
+    for s in range(3):
+        ora.step(dt)
+        gpu.step(dt)
+        err = max_var_rel_l2(p.interior(gpu.conserved()), p.interior(ora.conserved()))
+        assert err < STEP_TOL, f"step {s}: rel L2 {err}"
+    assert gpu.error_word() == 0
+
+
+def test_cfl_steps_match(oracle_mod):
+    """device-computed CFL dt, several steps with graph replay"""
+    p = perturb(small_c1(), dv=1.0)
+    gpu = MeshBlock(p, graph=True)
+    ora = oracle_mod.OracleBlock(p)
+    for s in range(4):
+        dto = ora.new_dt()
+        dtg = gpu.new_dt()
+        assert abs(dtg - dto) <= 1e-11 * dto
+        ora.step(dto)
+        gpu.step()
+    err = max_var_rel_l2(p.interior(gpu.conserved()), p.interior(ora.conserved()))
+    assert err < STEP_TOL
+
+
+def saturated_cells(th, n, seed):
+    """cells around saturation: T in [230, 310] K, total water 0.5-2x saturation"""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ny = th.ny
+    T = rng.uniform(230.0, 310.0, n)
+    p = rng.uniform(3e4, 1.0e5, n)
+    rho_guess = p / (th.rd * T)
+    es = thermo.svp(th, 0, T)
+    rv = th.rd * (1 + th.inv_mu_ratio_m1[0])
+    qs = es / (rho_guess * rv * T)
+    qt = qs * rng.uniform(0.5, 2.0, n)
+    w = np.zeros((5 + ny, n))
+    w[0] = rho_guess
+    w[1] = qt  # all water starts as vapour (super- or sub-saturated)
+    w[1 + ny:4 + ny] = rng.uniform(-10, 10, (3, n))
+    feps = thermo.feps_of(th, w[1:1 + ny])
+    w[4 + ny] = rho_guess * th.rd * feps * T
+    return thermo.prim_to_cons(th, w)
+
+
+def test_saturation_adjust(oracle_mod):
+    import torch
+    th = thermo.earth_moist()
+    n = 20000
+    u = saturated_cells(th, n, seed=5)
+    ref = u.copy()
+    t_ref, it_ref, fl_ref = oracle_mod.satadj(th, ref)
+    d = torch.from_numpy(u.copy()).cuda()
+    t = torch.zeros(n, dtype=torch.float64, device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    st = torch.zeros(4, dtype=torch.int64, device="cuda")
+    o = SatOpts(1e-8, 30, 0)
+    torch.cuda.synchronize()
+    check(load().canoe_saturation_adjust(ctypes.byref(th), ctypes.byref(o), d.data_ptr(), n,
+                                          None, t.data_ptr(), it.data_ptr(), st.data_ptr(), None))
+    torch.cuda.synchronize()
+    got = d.cpu().numpy()
+    assert np.max(np.abs(t.cpu().numpy() - t_ref)) < 1e-9
+    for s in range(1, 4):
+        assert np.max(np.abs(got[s] - ref[s])) <= 1e-12 * np.abs(ref[1:4]).max()
+    # dry air, momentum and energy untouched; total water conserved
+    np.testing.assert_array_equal(got[0], u[0])
+    np.testing.assert_array_equal(got[4:], u[4:])
+    tw0 = u[1:4].sum(axis=0)
+    tw1 = got[1:4].sum(axis=0)
+    assert np.max(np.abs(tw1 - tw0) / tw0) < 1e-14
+    stats = st.cpu().numpy()
+    assert stats[0] == n and stats[3] == 0
+    assert (it.cpu().numpy() == it_ref).mean() > 0.99
+
+
+def test_conservation_moist_column_physics():
+    """mass and total water conserved to FP64 roundoff over several full steps
+    (periodic sides, reflecting top and bottom, saturation adjustment on)"""
+    p = perturb(small_c2(nx1=32, nx2=24, nx3=24, x1max=4000.0, x2max=6000.0, x3max=6000.0),
+                dv=1.0)
+    gpu = MeshBlock(p)
+    u0 = p.interior(gpu.conserved())
+    m0 = u0[:4].sum()
+    w0 = u0[1:4].sum()
+    for _ in range(5):
+        gpu.step()
+    u1 = p.interior(gpu.conserved())
+    assert abs(u1[:4].sum() - m0) / m0 < 1e-13
+    assert abs(u1[1:4].sum() - w0) / w0 < 1e-12
+    assert gpu.error_word() == 0
+
+
+def test_error_word_flags_injected_nan():
+    """host-side fault injection: a NaN planted in the conserved state is
+    reported through the device error word"""
+    p = small_c1()
+    u = p.u.copy()
+    p.interior(u)[0, 0, 5, 7] = np.nan
+    p.u = u
+    gpu = MeshBlock(p)
+    bits = gpu.error_word()
+    assert bits & 4
