@@ -45,17 +45,17 @@ int cuda_status(cudaError_t e, const char *what);
 // eos.cu).  `dtp` points at the device copy of the step's dt; every kernel
 // multiplies it by the stage's beta so that a step can be captured in a CUDA
 // graph without baking dt in.
-int launch_flux_x1(const Geom &g, const canoe_thermo_t &th, int recon, int rs,
-                   int precision, const double *w, double *du, const double *dtp,
-                   double beta, double *flx_out, cudaStream_t st);
+// x1 pencil kernel (column.cuh): mode 0 fluxes only (writes flx_out and the
+// x1 part of du), 1 full stage (fluxes + implicit solve + RK update of u),
+// 2 implicit solve of du only
+int launch_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs,
+                 int implicit_flag, int mode, const double *w, double *du, double *u,
+                 double *u1, const double *dtp, const Stage &s, int stage,
+                 double *flx_out, cudaStream_t st);
 int launch_flux_x23(int dir, const Geom &g, const canoe_thermo_t &th, int recon,
                     int rs, int precision, const double *w, double *du,
                     const double *dtp, double beta, double *flx_out,
                     cudaStream_t st);
-int launch_update(const Geom &g, const canoe_thermo_t &th, int implicit_flag,
-                  const double *w, double *du, double *u, double *u1,
-                  const double *dtp, const Stage &s, int stage, int mode,
-                  double *scratch, cudaStream_t st);
 int launch_cons_to_prim(const Geom &g, const canoe_thermo_t &th, const double *u,
                         double *w, uint32_t *err, unsigned long long *dt_acc,
                         double cfl, int implicit_flag, cudaStream_t st);
@@ -66,9 +66,8 @@ int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                   const double *t_guess, double *t_out, int32_t *iters,
                   unsigned long long *stats, cudaStream_t st);
 
-// update modes for launch_update
-enum UpdateMode { kUpdateRK = 0, kUpdateCorrectOnly = 1 };
+// raise a kernel's dynamic shared-memory limit once per (kernel, size)
+int ensure_smem(const void *kernel, size_t bytes);
 
-size_t implicit_scratch_doubles(const Geom &g, int implicit_flag);
 
 }  // namespace cb

@@ -1,0 +1,207 @@
+// blockmat.cuh -- small dense block algebra of the implicit vertical solver
+// (canoe src/snap/implicit/flux_decomposition.hpp): flux Jacobian, the
+// Roe-averaged |A| = R |Lambda| R^-1, 3x3 / 5x5 inverses and products.
+// N = 3 is the reduced (rho, m1, E) system of PartialCorrection, N = 5 the
+// full system of FullCorrection.
+#pragma once
+
+#include "block.cuh"
+
+namespace cb {
+
+template <int N>
+struct M {
+  double a[N][N];
+};
+template <int N>
+struct V {
+  double a[N];
+};
+
+template <int N>
+__device__ __forceinline__ M<N> mm(const M<N> &x, const M<N> &y) {
+  M<N> r;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      double s = 0.;
+#pragma unroll
+      for (int k = 0; k < N; ++k) s += x.a[i][k] * y.a[k][j];
+      r.a[i][j] = s;
+    }
+  return r;
+}
+
+template <int N>
+__device__ __forceinline__ V<N> mv(const M<N> &x, const V<N> &y) {
+  V<N> r;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < N; ++k) s += x.a[i][k] * y.a[k];
+    r.a[i] = s;
+  }
+  return r;
+}
+
+__device__ __forceinline__ M<3> inv(const M<3> &m) {
+  const double(*a)[3] = m.a;
+  double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+  double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+  double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+  double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+  double id = 1. / det;
+  M<3> r;
+  r.a[0][0] = c00 * id;
+  r.a[1][0] = c01 * id;
+  r.a[2][0] = c02 * id;
+  r.a[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id;
+  r.a[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id;
+  r.a[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id;
+  r.a[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id;
+  r.a[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id;
+  r.a[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id;
+  return r;
+}
+
+// Gauss-Jordan with partial pivoting
+__device__ __forceinline__ M<5> inv(const M<5> &m) {
+  double a[5][10];
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      a[i][j] = m.a[i][j];
+      a[i][5 + j] = (i == j) ? 1. : 0.;
+    }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    int p = c;
+#pragma unroll
+    for (int r = c + 1; r < 5; ++r)
+      if (fabs(a[r][c]) > fabs(a[p][c])) p = r;
+    if (p != c) {
+#pragma unroll
+      for (int r = c + 1; r < 5; ++r)
+        if (r == p)
+#pragma unroll
+          for (int j = 0; j < 10; ++j) {
+            double t = a[c][j];
+            a[c][j] = a[r][j];
+            a[r][j] = t;
+          }
+    }
+    double ip = 1. / a[c][c];
+#pragma unroll
+    for (int j = 0; j < 10; ++j) a[c][j] *= ip;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      if (r == c) continue;
+      double f = a[r][c];
+      if (f != 0.)
+#pragma unroll
+        for (int j = 0; j < 10; ++j) a[r][j] -= f * a[c][j];
+    }
+  }
+  M<5> r;
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int j = 0; j < 5; ++j) r.a[i][j] = a[i][5 + j];
+  return r;
+}
+
+// row / column selection of the reduced (partial) system: (rho, m1, E)
+template <int N>
+__device__ __forceinline__ constexpr int sel(int r) {
+  return N == 5 ? r : (r == 2 ? 4 : r);
+}
+
+// FluxJacobian (flux_decomposition.hpp:102-120), reduced to N x N
+template <int N, int NY>
+__device__ __forceinline__ void jacobian(M<N> &d, double gm1, const double *w) {
+  using S = Slots<NY>;
+  double v1 = w[S::IVX], v2 = w[S::IVY], v3 = w[S::IVZ];
+  double rho = w[0], pres = w[S::IPR];
+  double s2 = v1 * v1 + v2 * v2 + v3 * v3;
+  double c1 = ((gm1 - 1) * s2 / 2 - (gm1 + 1) / gm1 * pres / rho) * v1;
+  double c2 = (gm1 + 1) / gm1 * pres / rho + s2 / 2 - gm1 * v1 * v1;
+  const double f[5][5] = {{0, 1., 0., 0., 0.},
+                          {gm1 * s2 / 2 - v1 * v1, (2. - gm1) * v1, -gm1 * v2, -gm1 * v3, gm1},
+                          {-v1 * v2, v2, v1, 0., 0.},
+                          {-v1 * v3, v3, 0., v1, 0.},
+                          {c1, c2, -gm1 * v2 * v1, -gm1 * v3 * v1, (gm1 + 1) * v1}};
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int c = 0; c < N; ++c) d.a[r][c] = f[sel<N>(r)][sel<N>(c)];
+}
+
+// |A| = R |Lambda| R^-1 at the face between cells with primitive states wl,
+// wr: RoeAverage (:34-67), SoundSpeed, Eigenvalue (:70-75), Eigenvector
+// (:78-99); only the N x N reduced block is formed.
+template <int N, int NY>
+__device__ __forceinline__ void abs_jacobian(M<N> &A, const canoe_thermo_t &th,
+                                             double gm1, const double *wl,
+                                             const double *wr) {
+  using S = Slots<NY>;
+  double prim[S::NV];
+  double sqrtdl = sqrt(wl[0]);
+  double sqrtdr = sqrt(wr[0]);
+  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  prim[0] = sqrtdl * sqrtdr;
+  prim[S::IVX] = (sqrtdl * wl[S::IVX] + sqrtdr * wr[S::IVX]) * isdlpdr;
+  prim[S::IVY] = (sqrtdl * wl[S::IVY] + sqrtdr * wr[S::IVY]) * isdlpdr;
+  prim[S::IVZ] = (sqrtdl * wl[S::IVZ] + sqrtdr * wr[S::IVZ]) * isdlpdr;
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) prim[n] = (sqrtdl * wl[n] + sqrtdr * wr[n]) * isdlpdr;
+  double el = wl[S::IPR] / gm1 + 0.5 * wl[0] *
+              (wl[S::IVX] * wl[S::IVX] + wl[S::IVY] * wl[S::IVY] + wl[S::IVZ] * wl[S::IVZ]);
+  double er = wr[S::IPR] / gm1 + 0.5 * wr[0] *
+              (wr[S::IVX] * wr[S::IVX] + wr[S::IVY] * wr[S::IVY] + wr[S::IVZ] * wr[S::IVZ]);
+  double hbar = ((el + wl[S::IPR]) / sqrtdl + (er + wr[S::IPR]) / sqrtdr) * isdlpdr;
+  prim[S::IPR] = (hbar - 0.5 * (prim[S::IVX] * prim[S::IVX] + prim[S::IVY] * prim[S::IVY] +
+                                prim[S::IVZ] * prim[S::IVZ])) *
+                 gm1 / (gm1 + 1.) * prim[0];
+  double cs = sound_speed<double, NY>(th, prim);
+  double r = prim[0], u = prim[S::IVX], v = prim[S::IVY], w = prim[S::IVZ],
+         p = prim[S::IPR];
+  double ke = 0.5 * (u * u + v * v + w * w);
+  double hp = (gm1 + 1.) / gm1 * p / r;
+  double h = hp + ke;
+  const double ihp = 1. / hp, i2hp = 0.5 * ihp, i2chp = i2hp / cs;
+  const double R[5][5] = {{1., 1., 1., 0., 0.},
+                          {u - cs, u, u + cs, 0., 0.},
+                          {v, v, v, 1., 0.},
+                          {w, w, w, 0., 1.},
+                          {h - u * cs, ke, h + u * cs, v, w}};
+  // R^-1 of Eigenvector (:94-98) with the divisions by hp, 2 hp and
+  // 2 cs hp taken as reciprocals
+  const double Ri[5][5] = {
+      {(cs * ke + u * hp) * i2chp, (-hp - cs * u) * i2chp, -v * i2hp, -w * i2hp, i2hp},
+      {(hp - ke) * ihp, u * ihp, v * ihp, w * ihp, -ihp},
+      {(cs * ke - u * hp) * i2chp, (hp - cs * u) * i2chp, -v * i2hp, -w * i2hp, i2hp},
+      {-v, 0., 1., 0., 0.},
+      {-w, 0., 0., 1., 0.}};
+  const double lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
+#pragma unroll
+  for (int a = 0; a < N; ++a)
+#pragma unroll
+    for (int b = 0; b < N; ++b) {
+      double s = 0.;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) s += (R[sel<N>(a)][k] * lam[k]) * Ri[k][sel<N>(b)];
+      A.a[a][b] = s;
+    }
+}
+
+template <int NY>
+__device__ __forceinline__ void load_w(const Geom &g, const double *__restrict__ w,
+                                       int64_t base, int i, double *out) {
+#pragma unroll
+  for (int n = 0; n < Slots<NY>::NV; ++n) out[n] = w[n * g.sv + base + i];
+}
+
+}  // namespace cb

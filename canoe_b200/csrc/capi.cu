@@ -7,10 +7,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
-#include "block.cuh"
+#include "column.cuh"
 
 namespace cb {
 
@@ -23,6 +25,19 @@ void set_error(const std::string &msg) { g_last_error = msg; }
 int cuda_status(cudaError_t e, const char *what) {
   g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
   return CANOE_ERR_CUDA;
+}
+
+int ensure_smem(const void *kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void *, size_t> done;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find(kernel);
+  if (it != done.end() && it->second >= bytes) return 0;
+  if (bytes > 48 * 1024)
+    CB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes));
+  done[kernel] = bytes;
+  return 0;
 }
 
 namespace {
@@ -167,10 +182,6 @@ static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullpt
   for (int s = 0; s < 3; ++s) {
     const Stage &sg = kRK3[s];
     CB_MARK(-1);
-    if ((rc = launch_flux_x1(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.precision,
-                             b->d_w, b->d_du, b->d_dt, sg.beta, nullptr, b->st)))
-      return rc;
-    CB_MARK(0);
     if (g.f2 && (rc = launch_flux_x23(1, g, b->th, b->cfg.recon, b->cfg.rsolver,
                                       b->cfg.precision, b->d_w, b->d_du, b->d_dt, sg.beta,
                                       nullptr, b->st)))
@@ -181,10 +192,11 @@ static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullpt
                                       nullptr, b->st)))
       return rc;
     CB_MARK(2);
-    if ((rc = launch_update(g, b->th, b->cfg.implicit_flag, b->d_w, b->d_du, b->d_u,
-                            b->d_u1, b->d_dt, sg, s, kUpdateRK, b->d_scr, b->st)))
+    if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                           kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt, sg, s,
+                           nullptr, b->st)))
       return rc;
-    CB_MARK(3);
+    CB_MARK(0);
     if (s == 2 && b->cfg.satadj && b->th.ny > 0) {
       canoe_satadj_opts_t o{1e-8, 30, 0};
       const int64_t nin = (int64_t)g.nx1 * g.nx2 * g.nx3;
@@ -346,8 +358,6 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
   if ((e = cudaMalloc(&b->d_dt, 2 * sizeof(double)))) return fail(e, "cudaMalloc dt");
   if ((e = cudaMalloc(&b->d_dtacc, sizeof(unsigned long long)))) return fail(e, "cudaMalloc dtacc");
   if ((e = cudaMalloc(&b->d_err, sizeof(uint32_t)))) return fail(e, "cudaMalloc err");
-  size_t ns = implicit_scratch_doubles(g, cfg->implicit_flag);
-  if (ns && (e = cudaMalloc(&b->d_scr, ns * sizeof(double)))) return fail(e, "cudaMalloc scratch");
   if ((e = cudaMemset(b->d_u, 0, bytes))) return fail(e, "cudaMemset u");
   if ((e = cudaMemset(b->d_w, 0, bytes))) return fail(e, "cudaMemset w");
   if ((e = cudaMemset(b->d_u1, 0, bytes))) return fail(e, "cudaMemset u1");
@@ -435,15 +445,17 @@ int canoe_block_calculate_fluxes(canoe_block_t b, double *f1, double *f2, double
     return CANOE_ERR_ARG;
   }
   const Geom &g = b->g;
+  const Stage one{0., 1., 1.};
   int rc;
-  if ((rc = launch_flux_x1(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.precision, b->d_w,
-                           b->d_du, b->d_dt, 1., f1, b->st)))
-    return rc;
   if (g.f2 && (rc = launch_flux_x23(1, g, b->th, b->cfg.recon, b->cfg.rsolver,
                                     b->cfg.precision, b->d_w, b->d_du, b->d_dt, 1., f2, b->st)))
     return rc;
   if (g.f3 && (rc = launch_flux_x23(2, g, b->th, b->cfg.recon, b->cfg.rsolver,
                                     b->cfg.precision, b->d_w, b->d_du, b->d_dt, 1., f3, b->st)))
+    return rc;
+  if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                         kColFluxOnly, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt, one, 1, f1,
+                         b->st)))
     return rc;
   CB_CUDA(cudaStreamSynchronize(b->st));
   return 0;
@@ -457,9 +469,10 @@ int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt) {
   if (!(b->cfg.implicit_flag & 1)) return 0;
   // the solve reads dt through the device dt slot: use slot 1 as a scratch
   CB_CUDA(cudaMemcpyAsync(b->d_dt + 1, &dt, sizeof(double), cudaMemcpyHostToDevice, b->st));
-  Stage s{0., 1., 1.};
-  int rc = launch_update(b->g, b->th, b->cfg.implicit_flag, b->d_w, d_du, b->d_u, b->d_u1,
-                         b->d_dt + 1, s, 1, kUpdateCorrectOnly, b->d_scr, b->st);
+  const Stage one{0., 1., 1.};
+  int rc = launch_x1col(b->g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                        kColSolveOnly, b->d_w, d_du, b->d_u, b->d_u1, b->d_dt + 1, one, 1,
+                        nullptr, b->st);
   if (rc) return rc;
   CB_CUDA(cudaStreamSynchronize(b->st));
   return 0;

@@ -266,6 +266,11 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
     fprev = fabs(f);
     if (fabs(dT) < o.tol) {
       converged = true;
+      // one polishing Newton step: the result no longer depends on which
+      // iterate first met the tolerance (cold vs warm start agree to roundoff)
+      sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+      T -= f / fp;
+      iters++;
       break;
     }
   }
@@ -284,6 +289,9 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
       iters++;
       if (fabs(dT) < o.tol || hi - lo < o.tol) {
         converged = true;
+        sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+        const double tp = T - f / fp;
+        if (tp > lo && tp < hi) T = tp;
         break;
       }
     }
@@ -295,7 +303,9 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
     if (v >= th.nvapor) break;
     const int ls = th.liq_slot[v], ss = th.ice_slot[v];
     if (ls < 0 || ss < 0) continue;
-    if (fabs(T - th.t3[v]) > 2. * o.tol + 1e-12 * th.t3[v]) continue;
+    // f is increasing in T, so the root sits on the jump iff
+    // f_ice(t3) < 0 < f_liquid(t3); only iterates ending near t3 can be there
+    if (fabs(T - th.t3[v]) > 1e-3) continue;
     double fl, fs, fpl, fps;
     double ql[NY + 1], qs_[NY + 1];
     sat_eval<NY>(th, c, th.t3[v], v, 0, fl, fpl, ql);

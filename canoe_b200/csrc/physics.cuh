@@ -67,8 +67,9 @@ __device__ __forceinline__ void ppm_cell(R qmm, R qm, R q0, R qp, R qpp, R &wL,
   R dm_m = ppm_slope(qmm, qm, q0);
   R dm_0 = ppm_slope(qm, q0, qp);
   R dm_p = ppm_slope(q0, qp, qpp);
-  wL = R(0.5) * (qm + q0) - (dm_0 - dm_m) / R(6);
-  wR = R(0.5) * (q0 + qp) - (dm_p - dm_0) / R(6);
+  constexpr R sixth = R(1) / R(6);
+  wL = R(0.5) * (qm + q0) - (dm_0 - dm_m) * sixth;
+  wR = R(0.5) * (q0 + qp) - (dm_p - dm_0) * sixth;
   if ((wR - q0) * (q0 - wL) <= R(0)) {
     wL = q0;
     wR = q0;

@@ -349,8 +349,9 @@ static void ppm_line(const double *q, int lo, int hi, double *ql, double *qr) {
     double dm_m = ppm_slope(q[c - 2], q[c - 1], q[c]);
     double dm_0 = ppm_slope(q[c - 1], q[c], q[c + 1]);
     double dm_p = ppm_slope(q[c], q[c + 1], q[c + 2]);
-    double wL = 0.5 * (q[c - 1] + q[c]) - (dm_0 - dm_m) / 6.;
-    double wR = 0.5 * (q[c] + q[c + 1]) - (dm_p - dm_0) / 6.;
+    const double sixth = 1. / 6.;
+    double wL = 0.5 * (q[c - 1] + q[c]) - (dm_0 - dm_m) * sixth;
+    double wR = 0.5 * (q[c] + q[c + 1]) - (dm_p - dm_0) * sixth;
     double w0 = q[c];
     if ((wR - w0) * (w0 - wL) <= 0.) {
       wL = w0;
@@ -614,7 +615,8 @@ void calculate_fluxes(Block &b) {
 }
 
 // Athena AddFluxDivergence for a Cartesian block (external; restated as the
-// finite-volume divergence), accumulated into du with weight wght = beta dt.
+// finite-volume divergence, face differences times the reciprocal widths),
+// accumulated into du with weight wght = beta dt.
 void add_flux_divergence(Block &b, double wght, std::vector<double> &du) {
   const int nc1 = b.nc1, nc2 = b.nc2;
 #pragma omp parallel for collapse(3) schedule(static)
@@ -623,14 +625,14 @@ void add_flux_divergence(Block &b, double wght, std::vector<double> &du) {
       for (int j = b.js; j <= b.je; ++j)
         for (int i = b.is; i <= b.ie; ++i) {
           size_t f1 = (((size_t)n * b.nc3 + k) * nc2 + j) * (nc1 + 1) + i;
-          double d = (b.flx1[f1 + 1] - b.flx1[f1]) / b.dx1f[i];
+          double d = (b.flx1[f1 + 1] - b.flx1[f1]) * (1. / b.dx1f[i]);
           if (b.f2) {
             size_t f2 = (((size_t)n * b.nc3 + k) * (nc2 + 1) + j) * nc1 + i;
-            d += (b.flx2[f2 + nc1] - b.flx2[f2]) / b.dx2;
+            d += (b.flx2[f2 + nc1] - b.flx2[f2]) * (1. / b.dx2);
           }
           if (b.f3) {
             size_t f3 = (((size_t)n * (b.nc3 + 1) + k) * nc2 + j) * nc1 + i;
-            d += (b.flx3[f3 + (size_t)nc2 * nc1] - b.flx3[f3]) / b.dx3;
+            d += (b.flx3[f3 + (size_t)nc2 * nc1] - b.flx3[f3]) * (1. / b.dx3);
           }
           du[b.idx(n, k, j, i)] -= wght * d;
         }

@@ -18,7 +18,8 @@
 // min(total, saturation).  Newton from a guess (cold start: the temperature
 // of the unadjusted state; warm start: a supplied guess) stops at |dT| < tol;
 // if the residual fails to drop, a bracketed Newton/bisection (the fallback)
-// finishes the solve.  A root on a liquid/ice jump at t3 is resolved by
+// finishes the solve.  One polishing Newton step follows convergence, so the
+// answer does not depend on the starting point beyond roundoff.  A root on a liquid/ice jump at t3 is resolved by
 // splitting the condensate between the two phases at T = t3.  Total energy
 // u[IEN] and dry density u[IDN] are untouched; only u[1..ny] change.
 // TEST INFRASTRUCTURE ONLY.
@@ -156,6 +157,9 @@ SatResult satadj_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
     fprev = std::fabs(e.f);
     if (std::fabs(dT) < o.tol) {
       r.converged = true;
+      e = evaluate(th, c, T);  // one polishing Newton step
+      T -= e.f / e.fp;
+      r.iters++;
       break;
     }
   }
@@ -175,6 +179,9 @@ SatResult satadj_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
       r.iters++;
       if (std::fabs(dT) < o.tol || hi - lo < o.tol) {
         r.converged = true;
+        e = evaluate(th, c, T);
+        double tp = T - e.f / e.fp;
+        if (tp > lo && tp < hi) T = tp;
         break;
       }
     }
@@ -183,7 +190,9 @@ SatResult satadj_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
   // a root on the liquid/ice jump of vapor v: split at T = t3
   for (int v = 0; v < th.nvapor; ++v) {
     if (th.liq_slot[v] < 0 || th.ice_slot[v] < 0) continue;
-    if (std::fabs(T - th.t3[v]) > 2. * o.tol + 1e-12 * th.t3[v]) continue;
+    // f is increasing in T, so the root sits on the jump iff
+    // f_ice(t3) < 0 < f_liquid(t3); only iterates ending near t3 can be there
+    if (std::fabs(T - th.t3[v]) > 1e-3) continue;
     Eval el = evaluate(th, c, th.t3[v], v, 0), es = evaluate(th, c, th.t3[v], v, 1);
     if ((el.f > 0.) == (es.f > 0.)) continue;
     double x = -es.f / (el.f - es.f);  // liquid share, f linear in x
