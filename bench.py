@@ -101,19 +101,20 @@ def make_problem(args, nx2=None, nx3=None):
 
 def algorithmic_bytes(nv, ny, ncell):
     """bytes per launch of each kernel class: inputs read once, outputs written
-    once, interior cells (SURVEY per-unit figures, 8-byte words)."""
+    once, interior cells, 8-byte words."""
     return {
-        "flux_x1": 16 * nv * ncell,            # read w, write du
-        "flux_x2": 24 * nv * ncell,            # read w, du; write du
-        "flux_x3": 24 * nv * ncell,
-        "update_implicit": (40 * nv + 8 * nv / 3.0) * ncell,  # read w,du,u,u1; write u (+u1)
-        "satadj": 8 * (nv + ny) * ncell,
-        "cons_to_prim": 16 * nv * ncell,
+        # x1 pencil: read w, du (x2/x3 part), u, u1; write u (+ u1 at stage 0)
+        "x1_pencil": (40 * nv + 8 * nv / 3.0) * ncell,
+        "flux_x2": 16 * nv * ncell,            # read w; write du
+        "flux_x3": 24 * nv * ncell,            # read w, du; write du
+        "satadj": 8 * (nv + ny) * ncell,       # read u; write u[1..ny]
+        "cons_to_prim": 16 * nv * ncell,       # read u; write w
     }
 
 
-CLASSES = ["flux_x1", "flux_x2", "flux_x3", "update_implicit", "satadj", "cons_to_prim", "dt"]
-LAUNCHES_PER_STEP = {"flux_x1": 3, "flux_x2": 3, "flux_x3": 3, "update_implicit": 3,
+# kernel classes timed by canoe_block_step_profile
+CLASSES = ["x1_pencil", "flux_x2", "flux_x3", "unused", "satadj", "cons_to_prim", "dt"]
+LAUNCHES_PER_STEP = {"x1_pencil": 3, "flux_x2": 3, "flux_x3": 3, "unused": 0,
                      "satadj": 1, "cons_to_prim": 3, "dt": 1}
 
 
@@ -158,7 +159,10 @@ def config_dict(args):
     return {"workload": f"C2 3-D moist convection LES {args.nx1}x{args.nx2}x{args.nx3}, "
                         "PPM + HLLC, implicit X1 partial 3x3, saturation adjustment each step",
             "cells": args.nx1 * args.nx2 * args.nx3, "nv": 8, "rk_stages": 3,
-            "precision": args.precision, "cfl": 0.8,
+            "precision": {"fp64": "FP64", "mixed": "FP32 fluxes on the hydrostatic "
+                          "perturbation, FP64 implicit / accumulation / saturation "
+                          "adjustment"}[args.precision],
+            "cfl": 0.8, "dt": "CFL step of the initial state, fixed",
             "l2_flush": "inputs larger than L2 (537 MB per state array)"}
 
 
@@ -171,7 +175,8 @@ def main():
     ap.add_argument("--nx1", type=int, default=128)
     ap.add_argument("--nx2", type=int, default=256)
     ap.add_argument("--nx3", type=int, default=256)
-    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="headline variant; the other one is timed alongside")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -192,55 +197,96 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from canoe_b200 import MeshBlock
-    from canoe_b200._abi import check, load
+    from canoe_b200._abi import FP32_PERTURBATION, FP64, check, load
     lib = load()
     p = make_problem(args)
     ncell = p.cfg.nx1 * p.cfg.nx2 * p.cfg.nx3
     nv, ny = p.nv, p.ny
     stream = torch.cuda.Stream()
-    blk = MeshBlock(p, graph=True)
-    check(lib.canoe_block_set_stream(blk.h, ctypes.c_void_p(stream.cuda_stream)))
-    launches = 0
+
+    def make_block(prec):
+        p.cfg.precision = prec
+        b = MeshBlock(p, graph=True)
+        check(lib.canoe_block_set_stream(b.h, ctypes.c_void_p(stream.cuda_stream)))
+        return b
+
+    blocks = {"fp64": make_block(FP64), "mixed": make_block(FP32_PERTURBATION)}
+    # both variants step with the CFL time step of the initial state
+    dt0 = blocks["fp64"].new_dt()
+    for b in blocks.values():
+        b.set_fixed_dt(dt0)
+    order = [args.precision] + [k for k in blocks if k != args.precision]
+    results, clocks = {}, None
     with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            blk.step()
-        stream.synchronize()
-        if dist:
-            dist.barrier()
-        sampler = ClockSampler(local)
-        sampler.start()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            blk.step()
-        e1.record(stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        clocks = sampler.stop()
-        launches = args.steps * sum(LAUNCHES_PER_STEP.values())
-        # per-kernel-class timing pass (events between launches, same stream)
-        prof = (ctypes.c_float * 7)()
-        nprof = max(2, min(args.steps, 5))
+        for name in order:
+            blk = blocks[name]
+            for _ in range(args.warmup):
+                blk.step()
+            stream.synchronize()
+            if dist:
+                dist.barrier()
+            sampler = ClockSampler(local) if name == args.precision else None
+            if sampler:
+                sampler.start()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                blk.step()
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            if sampler:
+                clocks = sampler.stop()
+            results[name] = {"ms": ms}
+    # L2 error of the mixed run against the FP64 run: both took warmup+steps
+    # steps of the same dt from the same state
+    from canoe_b200 import thermo as T_
+    wa, wb = p.interior(blocks["fp64"].primitive()), p.interior(blocks["mixed"].primitive())
+    ua, ub = p.interior(blocks["fp64"].conserved()), p.interior(blocks["mixed"].conserved())
+
+    def theta(w):
+        q = w[1:1 + ny]
+        T = w[4 + ny] / (w[0] * p.cfg.thermo.rd * T_.feps_of(p.cfg.thermo, q))
+        kap = (p.cfg.thermo.gammad - 1.0) / p.cfg.thermo.gammad
+        return T * (1.0e5 / w[4 + ny]) ** kap
+
+    def rl2(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    l2 = {"theta": rl2(theta(wb), theta(wa)),
+          "total_water": rl2(ub[1:1 + ny].sum(axis=0), ua[1:1 + ny].sum(axis=0)),
+          "steps": args.warmup + args.steps}
+    del wa, wb, ua, ub
+    # per-kernel-class timing pass of the headline variant
+    blk = blocks[args.precision]
+    prof = (ctypes.c_float * 7)()
+    nprof = max(2, min(args.steps, 5))
+    with torch.cuda.stream(stream):
         for _ in range(nprof):
             check(lib.canoe_block_step_profile(blk.h, -1.0, prof, 7))
         stream.synchronize()
+    launches = args.steps * sum(LAUNCHES_PER_STEP.values())
     err = blk.error_word()
-    t = torch.tensor([ms], device="cuda")
+    t = torch.tensor([results[args.precision]["ms"], results[order[1]]["ms"]], device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms, ms_other = float(t[0].item()), float(t[1].item())
     ms_step = ms / args.steps
     value = world * ncell * args.steps / (ms * 1e-3)
+    other = {"variant": order[1], "value": world * ncell * args.steps / (ms_other * 1e-3),
+             "ms_per_step": ms_other / args.steps}
 
     # roofline of the dominant kernel class
     hbm, peak_kind = peaks()
     abytes = algorithmic_bytes(nv, ny, ncell)
     per_class = {}
     for c, name in enumerate(CLASSES):
-        tot = prof[c] / nprof
         nl = LAUNCHES_PER_STEP[name]
+        if nl == 0:
+            continue
+        tot = prof[c] / nprof
         per_class[name] = {"ms_per_step": tot, "ms_per_launch": tot / nl}
         if name in abytes and tot > 0:
             per_class[name]["gbs"] = abytes[name] / (tot / nl * 1e-3) / 1e9
@@ -250,12 +296,13 @@ def main():
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(dom)
+            traffic = json.load(open(tf)).get(args.precision, {}).get(dom)
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                "per_kernel": per_class}
+                "algorithmic_bytes_per_launch": abytes[dom], "per_kernel": per_class}
+    p.cfg.precision = blk.problem.cfg.precision
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -263,6 +310,7 @@ def main():
         hu = torch.empty(p.u.shape, dtype=torch.float64).pin_memory()
         hu.numpy()[...] = p.u
         ho = torch.empty(p.u.shape, dtype=torch.float64).pin_memory()
+        blk = blocks[args.precision]
         torch.cuda.synchronize()
         k = args.steps
         t0 = time.perf_counter()
@@ -290,8 +338,12 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded C2 initial state)",
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded C2 initial state)",
             "config": config_dict(args), "gpu_launches": launches,
+            "other_variant": other, "speedup_mixed_vs_fp64":
+                (value / other["value"]) if args.precision == "mixed" else other["value"] / value,
+            "l2_error_mixed_vs_fp64": l2,
             "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
             "error_word": err}
     print(json.dumps(line), flush=True)

@@ -62,6 +62,9 @@ class MeshBlock:
     def step(self, dt=-1.0):
         check(self.lib.canoe_block_step(self.h, float(dt)), "step")
 
+    def set_fixed_dt(self, dt):
+        check(self.lib.canoe_block_set_fixed_dt(self.h, float(dt)), "set_fixed_dt")
+
     def synchronize(self):
         check(self.lib.canoe_block_synchronize(self.h), "synchronize")
 

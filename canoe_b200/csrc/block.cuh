@@ -23,6 +23,9 @@ struct Geom {
   int64_t sv;  // stride between variables (nc3 * nc2 * nc1)
   double dx2, dx3;
   const double *x1f, *x1v, *dx1f;  // device arrays, nc1+1 / nc1 / nc1
+  // horizontally uniform reference pressure per x1 level (nc1): the FP32
+  // flux path works on p' = p - pref so that p ~ 1e5 never enters FP32
+  const double *pref;
 };
 
 // RK3 (SSPRK(3,3), Shu & Osher 1988) register weights per stage:
@@ -49,7 +52,7 @@ int cuda_status(cudaError_t e, const char *what);
 // x1 part of du), 1 full stage (fluxes + implicit solve + RK update of u),
 // 2 implicit solve of du only
 int launch_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs,
-                 int implicit_flag, int mode, const double *w, double *du, double *u,
+                 int implicit_flag, int precision, int mode, const double *w, double *du, double *u,
                  double *u1, const double *dtp, const Stage &s, int stage,
                  double *flx_out, cudaStream_t st);
 int launch_flux_x23(int dir, const Geom &g, const canoe_thermo_t &th, int recon,
@@ -59,6 +62,8 @@ int launch_flux_x23(int dir, const Geom &g, const canoe_thermo_t &th, int recon,
 int launch_cons_to_prim(const Geom &g, const canoe_thermo_t &th, const double *u,
                         double *w, uint32_t *err, unsigned long long *dt_acc,
                         double cfl, int implicit_flag, cudaStream_t st);
+int launch_level_mean_pressure(const Geom &g, int ny, const double *w, double *pref,
+                               cudaStream_t st);
 int launch_dt_finalize(double *d_dt, unsigned long long *dt_acc, double cfl,
                        double fixed_dt, cudaStream_t st);
 int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,

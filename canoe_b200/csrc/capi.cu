@@ -132,13 +132,14 @@ struct canoe_block {
   canoe_thermo_t th;
   double *d_u = nullptr, *d_w = nullptr, *d_u1 = nullptr, *d_du = nullptr;
   double *d_x1f = nullptr, *d_x1v = nullptr, *d_dx1f = nullptr;
-  double *d_scr = nullptr, *d_dt = nullptr;
+  double *d_scr = nullptr, *d_dt = nullptr, *d_pref = nullptr;
   unsigned long long *d_dtacc = nullptr;
   uint32_t *d_err = nullptr;
   cudaStream_t st = nullptr;
   bool own_stream = false;
   cudaGraphExec_t gexec = nullptr;
   bool graph = false;
+  double fixed_dt = 0.;  // > 0: every step uses this dt instead of the CFL one
   size_t nvals = 0;
 };
 
@@ -147,7 +148,7 @@ static int block_free(canoe_block *b) {
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
   for (void *p : {(void *)b->d_u, (void *)b->d_w, (void *)b->d_u1, (void *)b->d_du,
                   (void *)b->d_x1f, (void *)b->d_x1v, (void *)b->d_dx1f,
-                  (void *)b->d_scr, (void *)b->d_dt, (void *)b->d_dtacc,
+                  (void *)b->d_scr, (void *)b->d_dt, (void *)b->d_pref, (void *)b->d_dtacc,
                   (void *)b->d_err})
     if (p) cudaFree(p);
   if (b->own_stream && b->st) cudaStreamDestroy(b->st);
@@ -193,7 +194,7 @@ static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullpt
       return rc;
     CB_MARK(2);
     if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
-                           kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt, sg, s,
+                           b->cfg.precision, kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt, sg, s,
                            nullptr, b->st)))
       return rc;
     CB_MARK(0);
@@ -211,7 +212,7 @@ static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullpt
       return rc;
     CB_MARK(5);
   }
-  rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, 0., b->st);
+  rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, b->fixed_dt, b->st);
   if (rc) return rc;
   CB_MARK(6);
 #undef CB_MARK
@@ -285,9 +286,9 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
     set_error("unknown Riemann solver");
     return CANOE_ERR_ARG;
   }
-  if (cfg->precision != CANOE_FP64) {
-    set_error("only the FP64 path is available in this build");
-    return CANOE_ERR_UNSUPPORTED;
+  if (cfg->precision != CANOE_FP64 && cfg->precision != CANOE_FP32_PERTURBATION) {
+    set_error("precision must be CANOE_FP64 or CANOE_FP32_PERTURBATION");
+    return CANOE_ERR_ARG;
   }
   for (int i = 0; i < cfg->nx1; ++i)
     if (!(cfg->h_x1f[i + 1] > cfg->h_x1f[i])) {
@@ -356,6 +357,8 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
   if ((e = cudaMalloc(&b->d_x1v, g.nc1 * sizeof(double)))) return fail(e, "cudaMalloc x1v");
   if ((e = cudaMalloc(&b->d_dx1f, g.nc1 * sizeof(double)))) return fail(e, "cudaMalloc dx1f");
   if ((e = cudaMalloc(&b->d_dt, 2 * sizeof(double)))) return fail(e, "cudaMalloc dt");
+  if ((e = cudaMalloc(&b->d_pref, g.nc1 * sizeof(double)))) return fail(e, "cudaMalloc pref");
+  if ((e = cudaMemset(b->d_pref, 0, g.nc1 * sizeof(double)))) return fail(e, "cudaMemset pref");
   if ((e = cudaMalloc(&b->d_dtacc, sizeof(unsigned long long)))) return fail(e, "cudaMalloc dtacc");
   if ((e = cudaMalloc(&b->d_err, sizeof(uint32_t)))) return fail(e, "cudaMalloc err");
   if ((e = cudaMemset(b->d_u, 0, bytes))) return fail(e, "cudaMemset u");
@@ -375,6 +378,7 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
   g.x1f = b->d_x1f;
   g.x1v = b->d_x1v;
   g.dx1f = b->d_dx1f;
+  g.pref = b->d_pref;
   *out = b;
   return 0;
 }
@@ -414,6 +418,8 @@ int canoe_block_set_conserved(canoe_block_t b, const double *h_u) {
                                    b->cfg.cfl, b->cfg.implicit_flag, b->st))
     return rc;
   if (int rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, 0., b->st)) return rc;
+  // reference pressure profile of the FP32 flux path (fixed for the run)
+  if (int rc = launch_level_mean_pressure(b->g, b->th.ny, b->d_w, b->d_pref, b->st)) return rc;
   CB_CUDA(cudaStreamSynchronize(b->st));
   return 0;
 }
@@ -454,7 +460,7 @@ int canoe_block_calculate_fluxes(canoe_block_t b, double *f1, double *f2, double
                                     b->cfg.precision, b->d_w, b->d_du, b->d_dt, 1., f3, b->st)))
     return rc;
   if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
-                         kColFluxOnly, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt, one, 1, f1,
+                         b->cfg.precision, kColFluxOnly, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt, one, 1, f1,
                          b->st)))
     return rc;
   CB_CUDA(cudaStreamSynchronize(b->st));
@@ -471,7 +477,7 @@ int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt) {
   CB_CUDA(cudaMemcpyAsync(b->d_dt + 1, &dt, sizeof(double), cudaMemcpyHostToDevice, b->st));
   const Stage one{0., 1., 1.};
   int rc = launch_x1col(b->g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
-                        kColSolveOnly, b->d_w, d_du, b->d_u, b->d_u1, b->d_dt + 1, one, 1,
+                        b->cfg.precision, kColSolveOnly, b->d_w, d_du, b->d_u, b->d_u1, b->d_dt + 1, one, 1,
                         nullptr, b->st);
   if (rc) return rc;
   CB_CUDA(cudaStreamSynchronize(b->st));
@@ -481,6 +487,18 @@ int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt) {
 int canoe_block_use_graph(canoe_block_t b, int on) {
   if (!b) return CANOE_ERR_ARG;
   b->graph = on != 0;
+  return 0;
+}
+
+int canoe_block_set_fixed_dt(canoe_block_t b, double dt) {
+  if (!b) return CANOE_ERR_ARG;
+  b->fixed_dt = dt > 0. ? dt : 0.;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  if (int rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, b->fixed_dt, b->st)) return rc;
+  CB_CUDA(cudaStreamSynchronize(b->st));
   return 0;
 }
 

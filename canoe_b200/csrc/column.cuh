@@ -58,7 +58,10 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
   return s;
 }
 
-template <int NY, int RECON, int RS, int N, int MODE>
+// R = double: the FP64 path.  R = float: reconstruction and Riemann fluxes in
+// FP32 on the perturbation p' from the FP64 hydrostatic face pressure psf;
+// the divergence of psf and the gravity source are added in FP64.
+template <int NY, int RECON, int RS, int N, int MODE, typename R>
 __global__ void __launch_bounds__(128, 3)
     k_x1col(Geom g, canoe_thermo_t th, const double *__restrict__ w,
             double *__restrict__ du, double *__restrict__ u, double *__restrict__ u1,
@@ -84,23 +87,32 @@ __global__ void __launch_bounds__(128, 3)
   for (int n = 0; n < NV; ++n)
     for (int i = tid; i < nc1; i += nth) wp[n * nc1 + i] = w[n * g.sv + base + i];
 
+  constexpr bool PERT = sizeof(R) == 4;
   if constexpr (MODE != kColSolveOnly) {
-    double *q = un;                 // [NV][nc1] transformed copy, later F
-    double *WL = q + NV * nc1;      // [NV][nc1]
-    double *WR = WL + NV * nc1;     // [NV][nc1]
-    double *psf = WR + NV * nc1;    // [nc1+1]
-    double *psv = psf + nc1 + 1;    // [nc1]
-    double *gam = psv + nc1;        // [nc1]
-    double *F = q;                  // [NV][nx1+1]
+    R *q = reinterpret_cast<R *>(un);          // [NV][nc1] transformed copy, later F
+    R *WL = q + NV * nc1;                      // [NV][nc1]
+    R *WR = WL + NV * nc1;                     // [NV][nc1]
+    double *psf = un + (3 * NV * nc1 * (int)sizeof(R) + 7) / 8;  // [nc1+1]
+    double *psv = psf + nc1 + 1;               // [nc1]
+    double *gam = psv + nc1;                   // [nc1]
+    R *F = q;                                  // [NV][nx1+1]
+    // without gravity the FP32 path uses one constant reference pressure
+    const double pcst = (PERT && grav == 0.) ? g.pref[is] : 0.;
     for (int n = 0; n < NV; ++n)
-      for (int i = tid; i < nc1; i += nth) q[n * nc1 + i] = wp[n * nc1 + i];
+      for (int i = tid; i < nc1; i += nth) {
+        double v = wp[n * nc1 + i];
+        if (n == S::IPR) v -= pcst;
+        q[n * nc1 + i] = R(v);
+      }
     // P1
     if (grav != 0.) {
-      double *rho = q, *pre = q + S::IPR * nc1;
+      R *rho = q, *pre = q + S::IPR * nc1;
+      const double *rho0 = wp, *pre0 = wp + S::IPR * nc1;
       for (int i = tid; i < nc1; i += nth) psv[i] = g.dx1f[i];
       __syncthreads();
       if (tid == 0) {
         const double *dx = psv;
+        const double *rho = rho0, *pre = pre0;
         double RdTv = pre[ie] / rho[ie];
         double acc = pre[ie] * exp(grav * dx[ie] / (2 * RdTv));
         psf[ie + 1] = acc;
@@ -127,12 +139,12 @@ __global__ void __launch_bounds__(128, 3)
         double feps = 1.;
 #pragma unroll
         for (int n = 1; n <= NY; ++n)
-          if (n <= th.nvapor) feps += q[n * nc1 + i] * th.inv_mu_ratio_m1[n - 1];
+          if (n <= th.nvapor) feps += wp[n * nc1 + i] * th.inv_mu_ratio_m1[n - 1];
         double gm = th.rd * feps;
         psv[i] = pv;
         gam[i] = gm;
-        rho[i] = pre[i] / (rho[i] * gm);
-        pre[i] -= pv;
+        rho[i] = R(pre0[i] / (rho0[i] * gm));
+        pre[i] = R(pre0[i] - pv);
       }
       __syncthreads();
       if (tid == 0) {
@@ -153,44 +165,61 @@ __global__ void __launch_bounds__(128, 3)
     const int ncell = nx1 + 2;
     for (int t = tid; t < NV * ncell; t += nth) {
       const int n = t / ncell, c = is - 1 + t % ncell;
-      const double *qn = q + n * nc1;
-      double wl_, wr_;
+      const R *qn = q + n * nc1;
+      R wl_, wr_;
       if constexpr (RECON == CANOE_RECON_PPM)
         ppm_cell(qn[c - 2], qn[c - 1], qn[c], qn[c + 1], qn[c + 2], wl_, wr_);
       else
-        plm_cell_nu(qn[c - 1], qn[c], qn[c + 1], g.x1v[c - 1], g.x1v[c], g.x1v[c + 1],
-                    g.x1f[c], g.x1f[c + 1], wl_, wr_);
+        plm_cell_nu(qn[c - 1], qn[c], qn[c + 1], R(g.x1v[c - 1]), R(g.x1v[c]),
+                    R(g.x1v[c + 1]), R(g.x1f[c]), R(g.x1f[c + 1]), wl_, wr_);
       WL[n * nc1 + c] = wl_;
       WR[n * nc1 + c] = wr_;
     }
     __syncthreads();
     // P3 (F aliases q, which nobody reads after P2)
     for (int f = is + tid; f <= ie + 1; f += nth) {
-      double wl[NV], wr[NV], fx[NV];
+      R wl[NV], wr[NV], fx[NV];
 #pragma unroll
       for (int n = 0; n < NV; ++n) {
         wl[n] = WR[n * nc1 + f - 1];
         wr[n] = WL[n * nc1 + f];
       }
+      const double pf = grav != 0. ? psf[f] : pcst;
       if (grav != 0.) {
-        const double pf = psf[f];
         const double gamma = sqrt(gam[f] * gam[f - 1]);
-        double pr = wr[S::IPR] + pf;
-        if (pr < 0.) pr = pf;
-        wr[S::IPR] = pr;
-        wr[0] = pr / (wr[0] * gamma);
-        double pl = wl[S::IPR] + pf;
-        if (pl < 0.) pl = pf;
-        wl[S::IPR] = pl;
-        wl[0] = pl / (wl[0] * gamma);
+        if constexpr (PERT) {
+          // keep p' relative to psf(f); floor p = psf(f) as the reference does
+          R pr = wr[S::IPR], pl = wl[S::IPR];
+          if (R(pf) + pr < R(0)) pr = R(0);
+          if (R(pf) + pl < R(0)) pl = R(0);
+          wr[S::IPR] = pr;
+          wl[S::IPR] = pl;
+          wr[0] = (R(pf) + pr) / (wr[0] * R(gamma));
+          wl[0] = (R(pf) + pl) / (wl[0] * R(gamma));
+        } else {
+          double pr = wr[S::IPR] + pf;
+          if (pr < 0.) pr = pf;
+          wr[S::IPR] = pr;
+          wr[0] = pr / (wr[0] * gamma);
+          double pl = wl[S::IPR] + pf;
+          if (pl < 0.) pl = pf;
+          wl[S::IPR] = pl;
+          wl[0] = pl / (wl[0] * gamma);
+        }
       }
-      riemann<double, NY, RS, 0>(th, wl, wr, fx);
+      if constexpr (PERT)
+        riemann_pert<R, NY, RS, 0>(th, wl, wr, R(pf), fx);
+      else
+        riemann<R, NY, RS, 0>(th, wl, wr, fx);
 #pragma unroll
       for (int n = 0; n < NV; ++n) F[n * (nx1 + 1) + (f - is)] = fx[n];
       if constexpr (MODE == kColFluxOnly) {
 #pragma unroll
-        for (int n = 0; n < NV; ++n)
-          fout[(((int64_t)n * g.nc3 + k) * g.nc2 + j) * (nc1 + 1) + f] = fx[n];
+        for (int n = 0; n < NV; ++n) {
+          double v = fx[n];
+          if (PERT && n == S::IVX) v += pf;  // report the full flux
+          fout[(((int64_t)n * g.nc3 + k) * g.nc2 + j) * (nc1 + 1) + f] = v;
+        }
       }
     }
     __syncthreads();
@@ -201,12 +230,14 @@ __global__ void __launch_bounds__(128, 3)
       double fm0 = 0., fm1 = 0.;
 #pragma unroll
       for (int n = 0; n <= NY; ++n) {
-        fm0 += F[n * (nx1 + 1) + f0];
-        fm1 += F[n * (nx1 + 1) + f0 + 1];
+        fm0 += (double)F[n * (nx1 + 1) + f0];
+        fm1 += (double)F[n * (nx1 + 1) + f0 + 1];
       }
 #pragma unroll
       for (int n = 0; n < NV; ++n) {
-        double d = (F[n * (nx1 + 1) + f0 + 1] - F[n * (nx1 + 1) + f0]) * idx;
+        double d = ((double)F[n * (nx1 + 1) + f0 + 1] - (double)F[n * (nx1 + 1) + f0]) * idx;
+        // FP32 path: the momentum flux lacks psf, whose divergence is FP64
+        if (PERT && n == S::IVX && grav != 0.) d += (psf[i + 1] - psf[i]) * idx;
         double v = -(wght * d);
         if (n == S::IVX) v += wght * grav * wp[i];
         if (n == S::IPR) v += wght * grav * 0.5 * (fm0 + fm1);
@@ -449,11 +480,11 @@ __global__ void __launch_bounds__(128, 3)
 }
 
 // launcher for one NY (instantiated in column_ny*.cu)
-template <int NY>
-int run_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int flag,
-              int mode, const double *w, double *du, double *u, double *u1,
-              const double *dtp, const Stage &s, int stage, double *fout,
-              cudaStream_t st) {
+template <int NY, typename R>
+int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int flag,
+                int mode, const double *w, double *du, double *u, double *u1,
+                const double *dtp, const Stage &s, int stage, double *fout,
+                cudaStream_t st) {
   const int nimpl = (mode == kColFluxOnly || !(flag & 1)) ? 0 : ((flag & 8) ? 5 : 3);
   if (mode == kColSolveOnly && nimpl == 0) return 0;
   const ColSmem L = col_smem(5 + NY, g.nc1, g.nx1, nimpl);
@@ -471,16 +502,28 @@ int run_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int fl
   };
   const bool ppm = recon == CANOE_RECON_PPM, hllc = rs == CANOE_RSOLVER_HLLC;
 #define CB_COL(NIMPL, MODE)                                                        \
-  (ppm ? (hllc ? go(k_x1col<NY, 3, 1, NIMPL, MODE>) : go(k_x1col<NY, 3, 0, NIMPL, MODE>)) \
-       : (hllc ? go(k_x1col<NY, 2, 1, NIMPL, MODE>) : go(k_x1col<NY, 2, 0, NIMPL, MODE>)))
+  (ppm ? (hllc ? go(k_x1col<NY, 3, 1, NIMPL, MODE, R>) : go(k_x1col<NY, 3, 0, NIMPL, MODE, R>)) \
+       : (hllc ? go(k_x1col<NY, 2, 1, NIMPL, MODE, R>) : go(k_x1col<NY, 2, 0, NIMPL, MODE, R>)))
   if (mode == kColFluxOnly) return CB_COL(0, kColFluxOnly);
   if (mode == kColSolveOnly)
-    return nimpl == 3 ? go(k_x1col<NY, 3, 1, 3, kColSolveOnly>)
-                      : go(k_x1col<NY, 3, 1, 5, kColSolveOnly>);
+    return nimpl == 3 ? go(k_x1col<NY, 3, 1, 3, kColSolveOnly, double>)
+                      : go(k_x1col<NY, 3, 1, 5, kColSolveOnly, double>);
   if (nimpl == 0) return CB_COL(0, kColStep);
   if (nimpl == 3) return CB_COL(3, kColStep);
   return CB_COL(5, kColStep);
 #undef CB_COL
+}
+
+template <int NY>
+int run_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int flag,
+              int prec, int mode, const double *w, double *du, double *u, double *u1,
+              const double *dtp, const Stage &s, int stage, double *fout,
+              cudaStream_t st) {
+  if (prec == CANOE_FP32_PERTURBATION && mode != kColSolveOnly)
+    return run_x1col_p<NY, float>(g, th, recon, rs, flag, mode, w, du, u, u1, dtp, s, stage,
+                                  fout, st);
+  return run_x1col_p<NY, double>(g, th, recon, rs, flag, mode, w, du, u, u1, dtp, s, stage,
+                                 fout, st);
 }
 
 }  // namespace cb

@@ -2,7 +2,7 @@
 #include "column.cuh"
 
 namespace cb {
-template int run_x1col<2>(const Geom &, const canoe_thermo_t &, int, int, int, int,
+template int run_x1col<2>(const Geom &, const canoe_thermo_t &, int, int, int, int, int,
                              const double *, double *, double *, double *,
                              const double *, const Stage &, int, double *, cudaStream_t);
 }  // namespace cb

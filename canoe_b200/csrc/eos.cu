@@ -104,6 +104,30 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// horizontal mean of the pressure at every x1 level (ghosts included): the
+// reference profile of the FP32 flux path
+template <int NY>
+__global__ void k_level_mean_pressure(Geom g, const double *__restrict__ w,
+                                      double *__restrict__ pref) {
+  const int i = blockIdx.x;
+  const int ncol = g.nx2 * g.nx3;
+  double s = 0.;
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+    const int j = g.js + c % g.nx2, k = g.ks + c / g.nx2;
+    s += w[Slots<NY>::IPR * g.sv + (int64_t)k * g.sk + (int64_t)j * g.nc1 + i];
+  }
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+    pref[i] = t / ncol;
+  }
+}
+
 __global__ void k_dt_finalize(double *d_dt, unsigned long long *acc, double cfl,
                               double fixed_dt) {
   if (fixed_dt > 0.)
@@ -392,6 +416,22 @@ int launch_cons_to_prim(const Geom &g, const canoe_thermo_t &th, const double *u
     case 2: k_cons_to_prim<2><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
     case 3: k_cons_to_prim<3><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
     case 6: k_cons_to_prim<6><<<nb, 256, 0, st>>>(g, th, u, w, err, dt_acc, cfl, imp); break;
+    default:
+      set_error("unsupported number of mass-fraction slots");
+      return CANOE_ERR_UNSUPPORTED;
+  }
+  CB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_level_mean_pressure(const Geom &g, int ny, const double *w, double *pref,
+                               cudaStream_t st) {
+  switch (ny) {
+    case 0: k_level_mean_pressure<0><<<g.nc1, 256, 0, st>>>(g, w, pref); break;
+    case 1: k_level_mean_pressure<1><<<g.nc1, 256, 0, st>>>(g, w, pref); break;
+    case 2: k_level_mean_pressure<2><<<g.nc1, 256, 0, st>>>(g, w, pref); break;
+    case 3: k_level_mean_pressure<3><<<g.nc1, 256, 0, st>>>(g, w, pref); break;
+    case 6: k_level_mean_pressure<6><<<g.nc1, 256, 0, st>>>(g, w, pref); break;
     default:
       set_error("unsupported number of mass-fraction slots");
       return CANOE_ERR_UNSUPPORTED;

@@ -22,7 +22,10 @@ namespace {
 constexpr int TI = 32;  // tile width along i
 constexpr int TD = 8;   // tile length along the flux direction
 
-template <int NY, int RECON, int RS, int DIR, bool WF>
+// R = double: the FP64 path.  R = float: reconstruction and Riemann fluxes
+// in FP32 on p' = p - pref(i); pref is the same on both sides of an x2 / x3
+// face, so it cancels from the momentum-flux divergence exactly.
+template <int NY, int RECON, int RS, int DIR, bool WF, typename R>
 __global__ void __launch_bounds__(256)
     k_flux_x23(Geom g, canoe_thermo_t th, const double *__restrict__ w,
                double *__restrict__ du, const double *__restrict__ dtp,
@@ -31,11 +34,13 @@ __global__ void __launch_bounds__(256)
   constexpr int NV = S::NV;
   constexpr int QR = TD + 2 * NG;  // staged rows
   constexpr int RR = TD + 2;       // reconstructed cells
-  extern __shared__ double sm[];
-  double *q = sm;                  // [NV][QR][TI]
-  double *WL = q + NV * QR * TI;   // [NV][RR][TI]
-  double *WR = WL + NV * RR * TI;  // [NV][RR][TI]
-  double *F = q;                   // [NV][TD+1][TI]
+  constexpr bool PERT = sizeof(R) == 4;
+  extern __shared__ double sm_[];
+  R *sm = reinterpret_cast<R *>(sm_);
+  R *q = sm;                       // [NV][QR][TI]
+  R *WL = q + NV * QR * TI;        // [NV][RR][TI]
+  R *WR = WL + NV * RR * TI;       // [NV][RR][TI]
+  R *F = q;                        // [NV][TD+1][TI]
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i = g.is + blockIdx.x * TI + tx;
@@ -48,20 +53,24 @@ __global__ void __launch_bounds__(256)
   const int64_t sd = DIR == 1 ? g.nc1 : g.sk;
   const int64_t base = (DIR == 1 ? (int64_t)o * g.sk : (int64_t)o * g.nc1) + i;
 
+  const double pref = PERT ? g.pref[iok ? i : g.is] : 0.;
   // P0: stage cells d0-3 .. d0+nd+2
   for (int c = ty; c < nd + 2 * NG; c += blockDim.y) {
     const int64_t off = base + (int64_t)(d0 - NG + c) * sd;
 #pragma unroll
-    for (int n = 0; n < NV; ++n)
-      q[(n * QR + c) * TI + tx] = iok ? w[n * g.sv + off] : 1.;
+    for (int n = 0; n < NV; ++n) {
+      double v = iok ? w[n * g.sv + off] : 1.;
+      if (PERT && n == S::IPR) v = iok ? v - pref : 0.;
+      q[(n * QR + c) * TI + tx] = R(v);
+    }
   }
   __syncthreads();
   // P1: reconstruct cells d0-1 .. d0+nd (local c = 0 .. nd+1)
   for (int c = ty; c < nd + 2; c += blockDim.y) {
 #pragma unroll
     for (int n = 0; n < NV; ++n) {
-      const double *qc = q + (n * QR + c) * TI + tx;
-      double wl_, wr_;
+      const R *qc = q + (n * QR + c) * TI + tx;
+      R wl_, wr_;
       if constexpr (RECON == CANOE_RECON_PPM)
         ppm_cell(qc[0], qc[TI], qc[2 * TI], qc[3 * TI], qc[4 * TI], wl_, wr_);
       else
@@ -73,13 +82,16 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   // P2: faces d0 .. d0+nd (local f = 0 .. nd): left cell c = f, right c = f+1
   for (int f = ty; f <= nd; f += blockDim.y) {
-    double wl[NV], wr[NV], fx[NV];
+    R wl[NV], wr[NV], fx[NV];
 #pragma unroll
     for (int n = 0; n < NV; ++n) {
       wl[n] = WR[(n * RR + f) * TI + tx];
       wr[n] = WL[(n * RR + f + 1) * TI + tx];
     }
-    riemann<double, NY, RS, DIR>(th, wl, wr, fx);
+    if constexpr (PERT)
+      riemann_pert<R, NY, RS, DIR>(th, wl, wr, R(pref), fx);
+    else
+      riemann<R, NY, RS, DIR>(th, wl, wr, fx);
 #pragma unroll
     for (int n = 0; n < NV; ++n) F[(n * (TD + 1) + f) * TI + tx] = fx[n];
     if constexpr (WF) {
@@ -90,7 +102,9 @@ __global__ void __launch_bounds__(256)
           int64_t idx = DIR == 1
               ? (((int64_t)n * g.nc3 + o) * (g.nc2 + 1) + fd) * g.nc1 + i
               : (((int64_t)n * (g.nc3 + 1) + fd) * g.nc2 + o) * g.nc1 + i;
-          fout[idx] = fx[n];
+          double v = fx[n];
+          if (PERT && n == S::IVX + DIR) v += pref;  // report the full flux
+          fout[idx] = v;
         }
       }
     }
@@ -104,7 +118,8 @@ __global__ void __launch_bounds__(256)
     const int64_t off = base + (int64_t)(d0 + c) * sd;
 #pragma unroll
     for (int n = 0; n < NV; ++n) {
-      double d = (F[(n * (TD + 1) + c + 1) * TI + tx] - F[(n * (TD + 1) + c) * TI + tx]) * idx;
+      double d = ((double)F[(n * (TD + 1) + c + 1) * TI + tx] -
+                  (double)F[(n * (TD + 1) + c) * TI + tx]) * idx;
       if (DIR == 1)
         du[n * g.sv + off] = -(wght * d);  // x2 runs first: initialise du
       else
@@ -113,17 +128,17 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-template <int NY>
+template <int NY, typename R>
 size_t x23_smem() {
   constexpr int NV = 5 + NY;
-  return sizeof(double) * (size_t)NV * TI * ((TD + 2 * NG) + 2 * (TD + 2));
+  return sizeof(R) * (size_t)NV * TI * ((TD + 2 * NG) + 2 * (TD + 2));
 }
 
-template <int NY, int RECON, int RS, int DIR, bool WF>
+template <int NY, int RECON, int RS, int DIR, bool WF, typename R>
 int run_x23(const Geom &g, const canoe_thermo_t &th, const double *w, double *du,
             const double *dtp, double beta, double *fo, cudaStream_t st) {
-  auto kern = k_flux_x23<NY, RECON, RS, DIR, WF>;
-  size_t sm = x23_smem<NY>();
+  auto kern = k_flux_x23<NY, RECON, RS, DIR, WF, R>;
+  size_t sm = x23_smem<NY, R>();
   if (int rc = ensure_smem((const void *)kern, sm)) return rc;
   const int nd = DIR == 1 ? g.nx2 : g.nx3;
   const int no = DIR == 1 ? g.nx3 : g.nx2;
@@ -147,12 +162,12 @@ int run_x23(const Geom &g, const canoe_thermo_t &th, const double *w, double *du
       return CANOE_ERR_UNSUPPORTED;                   \
   }
 
-template <int NY, int DIR>
+template <int NY, int DIR, typename RT>
 static int x23_dispatch(const Geom &g, const canoe_thermo_t &th, int recon, int rs,
                         const double *w, double *du, const double *dtp, double beta,
                         double *fo, cudaStream_t st) {
   const bool wf = fo != nullptr;
-#define CB_X23(R, S, W) return run_x23<NY, R, S, DIR, W>(g, th, w, du, dtp, beta, fo, st)
+#define CB_X23(R, S, W) return run_x23<NY, R, S, DIR, W, RT>(g, th, w, du, dtp, beta, fo, st)
   if (recon == CANOE_RECON_PPM) {
     if (rs == CANOE_RSOLVER_LMARS) { if (wf) CB_X23(3, 0, true); else CB_X23(3, 0, false); }
     else { if (wf) CB_X23(3, 1, true); else CB_X23(3, 1, false); }
@@ -166,11 +181,15 @@ static int x23_dispatch(const Geom &g, const canoe_thermo_t &th, int recon, int 
 int launch_flux_x23(int dir, const Geom &g, const canoe_thermo_t &th, int recon,
                     int rs, int precision, const double *w, double *du,
                     const double *dtp, double beta, double *fo, cudaStream_t st) {
-  (void)precision;
+  const bool f32 = precision == CANOE_FP32_PERTURBATION;
   if (dir == 1) {
-    CB_DISPATCH_NY(th.ny, (x23_dispatch<NY, 1>(g, th, recon, rs, w, du, dtp, beta, fo, st)));
+    if (f32)
+      CB_DISPATCH_NY(th.ny, (x23_dispatch<NY, 1, float>(g, th, recon, rs, w, du, dtp, beta, fo, st)));
+    CB_DISPATCH_NY(th.ny, (x23_dispatch<NY, 1, double>(g, th, recon, rs, w, du, dtp, beta, fo, st)));
   } else {
-    CB_DISPATCH_NY(th.ny, (x23_dispatch<NY, 2>(g, th, recon, rs, w, du, dtp, beta, fo, st)));
+    if (f32)
+      CB_DISPATCH_NY(th.ny, (x23_dispatch<NY, 2, float>(g, th, recon, rs, w, du, dtp, beta, fo, st)));
+    CB_DISPATCH_NY(th.ny, (x23_dispatch<NY, 2, double>(g, th, recon, rs, w, du, dtp, beta, fo, st)));
   }
 }
 

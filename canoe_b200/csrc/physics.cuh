@@ -263,6 +263,155 @@ __device__ __forceinline__ void riemann(const canoe_thermo_t &th, const R *wl,
     hllc<R, NY, DIR>(th, wl, wr, flx);
 }
 
+
+// ---------------------------------------------------------------------------
+// Perturbation form of the Riemann solvers for the FP32 path.  The pressure
+// slot of wl / wr holds p' = p - pref, with pref the FP64 hydrostatic
+// reference pressure at the face (the same on both sides).  The returned
+// normal-momentum flux excludes pref: F_ivx(p) = F'_ivx + pref exactly for
+// LMARS and, since sl + sr + sm = 1, for HLLC.  Absolute pressure enters only
+// where the solvers need it in relative terms (sound speeds, enthalpy).
+
+template <typename R, int NY, int DIR>
+__device__ __forceinline__ void lmars_pert(const canoe_thermo_t &th, const R *wli,
+                                           const R *wri, R pref, R *flx) {
+  using S = Slots<NY>;
+  constexpr int ivx = S::IVX + DIR;
+  constexpr int ivy = S::IVX + (DIR + 1) % 3;
+  constexpr int ivz = S::IVX + (DIR + 2) % 3;
+  constexpr int ipr = S::IPR;
+  const R pl = pref + wli[ipr], pr = pref + wri[ipr];
+  R kappal = R(1) / (get_gamma<R, NY>(th, wli) - R(1));
+  R kappar = R(1) / (get_gamma<R, NY>(th, wri) - R(1));
+  R hl = pl / wli[0] * (kappal + R(1)) +
+         R(0.5) * (wli[ivx] * wli[ivx] + wli[ivy] * wli[ivy] + wli[ivz] * wli[ivz]);
+  R hr = pr / wri[0] * (kappar + R(1)) +
+         R(0.5) * (wri[ivx] * wri[ivx] + wri[ivy] * wri[ivy] + wri[ivz] * wri[ivz]);
+  R rhobar = R(0.5) * (wli[0] + wri[0]);
+  R cbar = sqrt(R(0.5) * (R(1) + (R(1) / kappar + R(1) / kappal) / R(2)) * (pl + pr) / rhobar);
+  // pbar - pref and ubar from pressure differences only
+  R pbar = R(0.5) * (wli[ipr] + wri[ipr]) + R(0.5) * (rhobar * cbar) * (wli[ivx] - wri[ivx]);
+  R ubar = R(0.5) * (wli[ivx] + wri[ivx]) + R(0.5) / (rhobar * cbar) * (wli[ipr] - wri[ipr]);
+  R rdl = R(1), rdr = R(1);
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) {
+    rdl -= wli[n];
+    rdr -= wri[n];
+  }
+  const bool up = ubar > R(0);
+  R ws[S::NV];
+#pragma unroll
+  for (int n = 0; n < S::NV; ++n) ws[n] = up ? wli[n] : wri[n];
+  R rd = up ? rdl : rdr;
+  R h = up ? hl : hr;
+  flx[0] = ubar * ws[0] * rd;
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) flx[n] = ubar * ws[0] * ws[n];
+  flx[ivx] = ubar * ws[0] * ws[ivx] + pbar;
+  flx[ivy] = ubar * ws[0] * ws[ivy];
+  flx[ivz] = ubar * ws[0] * ws[ivz];
+  flx[ipr] = ubar * ws[0] * h;
+}
+
+template <typename R, int NY, int DIR>
+__device__ __forceinline__ void hllc_pert(const canoe_thermo_t &th, const R *wl, const R *wr,
+                                          R pref, R *flx) {
+  using S = Slots<NY>;
+  constexpr int IVX = S::IVX, IVY = S::IVY, IVZ = S::IVZ, IPR = S::IPR;
+  constexpr int ivx = IVX + DIR;
+  constexpr int ivy = IVX + (DIR + 1) % 3;
+  constexpr int ivz = IVX + (DIR + 2) % 3;
+  R wli[S::NV], wri[S::NV];
+  wli[0] = wl[0];
+  wri[0] = wr[0];
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) {
+    wli[n] = wl[n];
+    wri[n] = wr[n];
+  }
+  wli[IVX] = wl[ivx];
+  wli[IVY] = wl[ivy];
+  wli[IVZ] = wl[ivz];
+  wri[IVX] = wr[ivx];
+  wri[IVY] = wr[ivy];
+  wri[IVZ] = wr[ivz];
+  const R dpl = wl[IPR], dpr = wr[IPR];     // p' on each side
+  const R pl = pref + dpl, pr = pref + dpr;  // absolute, for relative uses
+  R gammal = get_gamma<R, NY>(th, wli);
+  R kappal = R(1) / (gammal - R(1));
+  R gammar = get_gamma<R, NY>(th, wri);
+  R kappar = R(1) / (gammar - R(1));
+  R cl = sqrt(gammal * pl / wli[0]);
+  R cr = sqrt(gammar * pr / wri[0]);
+  R KE_l = R(0.5) * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * wli[IVY] + wli[IVZ] * wli[IVZ]);
+  R KE_r = R(0.5) * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * wri[IVY] + wri[IVZ] * wri[IVZ]);
+  R el = pl * kappal + KE_l;
+  R er = pr * kappar + KE_r;
+  R rhoa = R(.5) * (wli[0] + wri[0]);
+  R ca = R(.5) * (cl + cr);
+  R dpmid = R(.5) * (dpl + dpr + (wli[IVX] - wri[IVX]) * rhoa * ca);
+  R pmid = pref + dpmid;
+  R ql = (dpmid <= dpl) ? R(1) : sqrt(R(1) + (gammal + R(1)) / (R(2) * gammal) * (pmid / pl - R(1)));
+  R qr = (dpmid <= dpr) ? R(1) : sqrt(R(1) + (gammar + R(1)) / (R(2) * gammar) * (pmid / pr - R(1)));
+  R al = wli[IVX] - cl * ql;
+  R ar = wri[IVX] + cr * qr;
+  R bp = ar > R(0) ? ar : R(TINY_NUMBER);
+  R bm = al < R(0) ? al : -R(TINY_NUMBER);
+  R vxl = wli[IVX] - al;
+  R vxr = wri[IVX] - ar;
+  R tl = dpl + vxl * wli[0] * wli[IVX];  // minus pref
+  R tr = dpr + vxr * wri[0] * wri[IVX];
+  R ml = wli[0] * vxl;
+  R mr = -(wri[0] * vxr);
+  R am = (tl - tr) / (ml + mr);
+  R dcp = (ml * tr + mr * tl) / (ml + mr);  // contact pressure minus pref
+  dcp = dcp > -pref ? dcp : -pref;
+  vxl = wli[IVX] - bm;
+  vxr = wri[IVX] - bp;
+  R rdl = R(1), rdr = R(1);
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) {
+    rdl -= wli[n];
+    rdr -= wri[n];
+  }
+  R sl, sr, sm;
+  if (am >= R(0)) {
+    sl = am / (am - bm);
+    sr = R(0);
+    sm = -bm / (am - bm);
+  } else {
+    sl = R(0);
+    sr = -am / (bp - am);
+    sm = bp / (bp - am);
+  }
+  R f[S::NV];
+  f[0] = sl * (wli[0] * vxl * rdl) + sr * (wri[0] * vxr * rdr);
+#pragma unroll
+  for (int n = 1; n <= NY; ++n)
+    f[n] = sl * (wli[0] * wli[n] * vxl) + sr * (wri[0] * wri[n] * vxr);
+  f[IVX] = sl * (wli[0] * wli[IVX] * vxl + dpl) + sr * (wri[0] * wri[IVX] * vxr + dpr) + sm * dcp;
+  f[IVY] = sl * (wli[0] * wli[IVY] * vxl) + sr * (wri[0] * wri[IVY] * vxr);
+  f[IVZ] = sl * (wli[0] * wli[IVZ] * vxl) + sr * (wri[0] * wri[IVZ] * vxr);
+  f[IPR] = sl * (el * vxl + pl * wli[IVX]) + sr * (er * vxr + pr * wri[IVX]) +
+           sm * (pref + dcp) * am;
+  flx[0] = f[0];
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) flx[n] = f[n];
+  flx[ivx] = f[IVX];
+  flx[ivy] = f[IVY];
+  flx[ivz] = f[IVZ];
+  flx[IPR] = f[IPR];
+}
+
+template <typename R, int NY, int RS, int DIR>
+__device__ __forceinline__ void riemann_pert(const canoe_thermo_t &th, const R *wl,
+                                             const R *wr, R pref, R *flx) {
+  if constexpr (RS == CANOE_RSOLVER_LMARS)
+    lmars_pert<R, NY, DIR>(th, wl, wr, pref, flx);
+  else
+    hllc_pert<R, NY, DIR>(th, wl, wr, pref, flx);
+}
+
 // ---------------------------------------------------------------------------
 // Ideal-moist EOS (snapy "U->W" / "W->U", restated): conserved u -> prim w.
 template <int NY>

@@ -204,6 +204,12 @@ int canoe_block_use_graph(canoe_block_t b, int on);
  * src/mesh_destroy.cpp:43-53). */
 int canoe_block_step_profile(canoe_block_t b, double dt, float *ms, int nclass);
 
+/* Pin the time step: dt > 0 makes every following step (graph replays
+ * included) use dt; dt <= 0 returns to the CFL step of
+ * canoe_block_new_dt.  The reference fixes dt only through its input file
+ * (Athena <time> dt); no direct counterpart. */
+int canoe_block_set_fixed_dt(canoe_block_t b, double dt);
+
 /* wait for the block's stream (steps are asynchronous) */
 int canoe_block_synchronize(canoe_block_t b);
 
