@@ -162,7 +162,8 @@ def config_dict(args):
             "precision": {"fp64": "FP64", "mixed": "FP32 fluxes on the hydrostatic "
                           "perturbation, FP64 implicit / accumulation / saturation "
                           "adjustment"}[args.precision],
-            "cfl": 0.8, "dt": "CFL step of the initial state, fixed",
+            "cfl": "0.8 split over the 2 horizontal directions (0.4 per direction)",
+            "dt": "CFL step of the initial state, fixed",
             "l2_flush": "inputs larger than L2 (537 MB per state array)"}
 
 

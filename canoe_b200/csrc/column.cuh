@@ -354,13 +354,19 @@ __global__ void __launch_bounds__(128, 3)
 #pragma unroll
       for (int e = 0; e < N; ++e) p[e] = v.a[e];
     };
+    // active rows are compacted onto the lowest threads so that a level
+    // with few rows occupies few warps
     int s = 1;
     for (; 2 * s - 1 < nx1; s *= 2) {
-      for (int r = tid; r < nx1; r += nth)
-        if ((r + 1) % (2 * s) == s) stm(blk + r * ROW, inv(ld(blk + r * ROW)));
+      const int ne = (nx1 + s) / (2 * s);  // eliminated rows r = s-1 + 2 s m
+      for (int m = tid; m < ne; m += nth) {
+        const int r = s - 1 + 2 * s * m;
+        stm(blk + r * ROW, inv(ld(blk + r * ROW)));
+      }
       __syncthreads();
-      for (int r = tid; r < nx1; r += nth) {
-        if ((r + 1) % (2 * s) != 0) continue;
+      const int nu = nx1 / (2 * s);  // surviving rows r = 2 s (m+1) - 1
+      for (int m = tid; m < nu; m += nth) {
+        const int r = 2 * s * (m + 1) - 1;
         double *row = blk + r * ROW;
         const double *lo = blk + (r - s) * ROW;
         M<N> a = ld(row), b = ld(row + NN), c = ld(row + 2 * NN);
@@ -409,8 +415,9 @@ __global__ void __launch_bounds__(128, 3)
     }
     __syncthreads();
     for (s /= 2; s >= 1; s /= 2) {
-      for (int r = tid; r < nx1; r += nth) {
-        if ((r + 1) % (2 * s) != s) continue;
+      const int ne = (nx1 + s) / (2 * s);
+      for (int m = tid; m < ne; m += nth) {
+        const int r = s - 1 + 2 * s * m;
         double *row = blk + r * ROW;
         V<N> rh = ldv(row + 3 * NN);
         if (r - s >= 0) {

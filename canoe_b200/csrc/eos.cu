@@ -314,8 +314,9 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
       if (fabs(dT) < o.tol || hi - lo < o.tol) {
         converged = true;
         sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+        // polish unless the step leaves the bracket (a root on a jump)
         const double tp = T - f / fp;
-        if (tp > lo && tp < hi) T = tp;
+        if (tp > lo - 2. * o.tol && tp < hi + 2. * o.tol) T = tp;
         break;
       }
     }

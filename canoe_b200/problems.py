@@ -83,8 +83,13 @@ def _embed(prob_shape, w_int, nx1, nx2, nx3):
 
 def bubble2d(nx1=150, nx2=100, x1max=1500.0, x2max=1000.0, dT=0.5, xc=500.0,
              zc=260.0, s=250.0, a=0.0, Ts=300.0, p0=1.0e5, grav=9.81,
-             gamma=1.4, cfl=0.8, recon=RECON_PLM, rsolver=RS_LMARS):
-    """C1: robert.cpp:72-114 with x1 vertical, nx3 = 1, reflecting walls."""
+             gamma=1.4, cfl=0.4, recon=RECON_PLM, rsolver=RS_LMARS):
+    """C1: robert.cpp:72-114 with x1 vertical, nx3 = 1, reflecting walls.
+
+    cfl: the time step is cfl x the per-direction minimum of dx / (|v| + c)
+    (patches/21.new_blockdt.patch); the configuration's Courant number 0.8
+    is split over the d = 2 directions that carry sound waves, because the
+    unsplit RK3 scheme grows grid-scale noise at 0.8 per direction."""
     th = T.dry(gammad=gamma, grav=-grav)
     Rd = th.rd
     cp = gamma / (gamma - 1.0) * Rd
@@ -168,8 +173,10 @@ def moist_profile(th, z, Ts=300.0, Ttop=200.0, ps=1.0e5, rh=0.8, zmoist=10.0e3,
 
 def moist3d(nx1=128, nx2=256, nx3=256, x1max=16.0e3, x2max=64.0e3, x3max=64.0e3,
             seed=20240601, noise=0.1, noise_depth=1.0e3, implicit_flag=1,
-            recon=RECON_PPM, rsolver=RS_HLLC, satadj=1, cfl=0.8, th=None):
-    """C2: 3-D moist convection LES initial state."""
+            recon=RECON_PPM, rsolver=RS_HLLC, satadj=1, cfl=0.4, th=None):
+    """C2: 3-D moist convection LES initial state.  cfl as in bubble2d: the
+    configuration's 0.8 split over the two horizontal directions (the
+    implicit x1 direction is limited by |v| only)."""
     th = th or T.earth_moist()
     ny = th.ny
     nv = 5 + ny

@@ -180,8 +180,9 @@ SatResult satadj_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
       if (std::fabs(dT) < o.tol || hi - lo < o.tol) {
         r.converged = true;
         e = evaluate(th, c, T);
+        // polish unless the step leaves the bracket (a root on a jump)
         double tp = T - e.f / e.fp;
-        if (tp > lo && tp < hi) T = tp;
+        if (tp > lo - 2. * o.tol && tp < hi + 2. * o.tol) T = tp;
         break;
       }
     }
