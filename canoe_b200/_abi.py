@@ -78,6 +78,24 @@ SIGNATURES = [
     ("canoe_block_step", c_int, [c_void_p, c_double]),
     ("canoe_block_new_dt", c_int, [c_void_p, POINTER(c_double)]),
     ("canoe_block_error_word", c_int, [c_void_p, POINTER(c_uint32)]),
+    ("canoe_block_set_mlp", c_int, [c_void_p, c_void_p]),
+    ("canoe_block_satadj_stats", c_int, [c_void_p, c_void_p]),
+    ("canoe_mlp_create", c_int, [ctypes.c_uint64, POINTER(c_void_p)]),
+    ("canoe_mlp_destroy", c_int, [c_void_p]),
+    ("canoe_mlp_nparams", c_int, []),
+    ("canoe_mlp_set_params", c_int, [c_void_p, c_void_p]),
+    ("canoe_mlp_get_params", c_int, [c_void_p, c_void_p]),
+    ("canoe_mlp_set_normalization", c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_float,
+                                            ctypes.c_float]),
+    ("canoe_mlp_get_normalization", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("canoe_mlp_loss_grad", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
+                                    c_void_p]),
+    ("canoe_mlp_adam_step", c_int, [c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, c_void_p]),
+    ("canoe_mlp_forward", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
+    ("canoe_saturation_adjust_learned", c_int, [POINTER(Thermo), POINTER(SatOpts), c_void_p,
+                                                c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                                c_void_p, c_void_p]),
 ]
 
 

@@ -66,10 +66,13 @@ int launch_level_mean_pressure(const Geom &g, int ny, const double *w, double *p
                                cudaStream_t st);
 int launch_dt_finalize(double *d_dt, unsigned long long *dt_acc, double cfl,
                        double fixed_dt, cudaStream_t st);
+struct MlpView;
 int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                   double *u, int64_t ncells, int64_t stride, const Geom *g,
                   const double *t_guess, double *t_out, int32_t *iters,
-                  unsigned long long *stats, cudaStream_t st);
+                  unsigned long long *stats, cudaStream_t st,
+                  const MlpView *mlp = nullptr, double *guess_out = nullptr);
+MlpView mlp_view(const struct canoe_mlp *m);
 
 // raise a kernel's dynamic shared-memory limit once per (kernel, size)
 int ensure_smem(const void *kernel, size_t bytes);

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "column.cuh"
+#include "mlp.cuh"
 
 namespace cb {
 
@@ -134,12 +135,14 @@ struct canoe_block {
   double *d_x1f = nullptr, *d_x1v = nullptr, *d_dx1f = nullptr;
   double *d_scr = nullptr, *d_dt = nullptr, *d_pref = nullptr;
   unsigned long long *d_dtacc = nullptr;
+  unsigned long long *d_sat = nullptr;  // saturation-adjustment statistics
   uint32_t *d_err = nullptr;
   cudaStream_t st = nullptr;
   bool own_stream = false;
   cudaGraphExec_t gexec = nullptr;
   bool graph = false;
   double fixed_dt = 0.;  // > 0: every step uses this dt instead of the CFL one
+  canoe_mlp_t mlp = nullptr;  // learned warm start of the saturation adjustment
   size_t nvals = 0;
 };
 
@@ -149,7 +152,7 @@ static int block_free(canoe_block *b) {
   for (void *p : {(void *)b->d_u, (void *)b->d_w, (void *)b->d_u1, (void *)b->d_du,
                   (void *)b->d_x1f, (void *)b->d_x1v, (void *)b->d_dx1f,
                   (void *)b->d_scr, (void *)b->d_dt, (void *)b->d_pref, (void *)b->d_dtacc,
-                  (void *)b->d_err})
+                  (void *)b->d_err, (void *)b->d_sat})
     if (p) cudaFree(p);
   if (b->own_stream && b->st) cudaStreamDestroy(b->st);
   delete b;
@@ -199,10 +202,12 @@ static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullpt
       return rc;
     CB_MARK(0);
     if (s == 2 && b->cfg.satadj && b->th.ny > 0) {
-      canoe_satadj_opts_t o{1e-8, 30, 0};
+      canoe_satadj_opts_t o{1e-8, 30, b->mlp ? 2 : 0};
       const int64_t nin = (int64_t)g.nx1 * g.nx2 * g.nx3;
+      MlpView mv;
+      if (b->mlp) mv = mlp_view(b->mlp);
       if ((rc = launch_satadj(b->th, o, b->d_u, nin, g.sv, &g, nullptr, nullptr, nullptr,
-                              nullptr, b->st)))
+                              b->d_sat, b->st, b->mlp ? &mv : nullptr, nullptr)))
         return rc;
       CB_MARK(4);
     }
@@ -361,6 +366,8 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
   if ((e = cudaMemset(b->d_pref, 0, g.nc1 * sizeof(double)))) return fail(e, "cudaMemset pref");
   if ((e = cudaMalloc(&b->d_dtacc, sizeof(unsigned long long)))) return fail(e, "cudaMalloc dtacc");
   if ((e = cudaMalloc(&b->d_err, sizeof(uint32_t)))) return fail(e, "cudaMalloc err");
+  if ((e = cudaMalloc(&b->d_sat, 4 * sizeof(unsigned long long)))) return fail(e, "cudaMalloc sat");
+  if ((e = cudaMemset(b->d_sat, 0, 4 * sizeof(unsigned long long)))) return fail(e, "cudaMemset sat");
   if ((e = cudaMemset(b->d_u, 0, bytes))) return fail(e, "cudaMemset u");
   if ((e = cudaMemset(b->d_w, 0, bytes))) return fail(e, "cudaMemset w");
   if ((e = cudaMemset(b->d_u1, 0, bytes))) return fail(e, "cudaMemset u1");
@@ -553,6 +560,44 @@ int canoe_block_new_dt(canoe_block_t b, double *dt_out) {
   CB_CUDA(cudaMemcpyAsync(dt_out, b->d_dt, sizeof(double), cudaMemcpyDeviceToHost, b->st));
   CB_CUDA(cudaStreamSynchronize(b->st));
   return 0;
+}
+
+int canoe_block_set_mlp(canoe_block_t b, canoe_mlp_t m) {
+  if (!b) return CANOE_ERR_ARG;
+  b->mlp = m;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return 0;
+}
+
+int canoe_block_satadj_stats(canoe_block_t b, unsigned long long *h_stats) {
+  if (!b || !h_stats) return CANOE_ERR_ARG;
+  CB_CUDA(cudaMemcpyAsync(h_stats, b->d_sat, 4 * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, b->st));
+  CB_CUDA(cudaMemsetAsync(b->d_sat, 0, 4 * sizeof(unsigned long long), b->st));
+  CB_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int canoe_saturation_adjust_learned(const canoe_thermo_t *th, const canoe_satadj_opts_t *opts,
+                                    canoe_mlp_t m, double *d_u, int64_t ncells,
+                                    double *d_t_out, int32_t *d_iters,
+                                    unsigned long long *d_stats, double *d_guess_out,
+                                    void *stream) {
+  if (!th || !opts || !m || !d_u || ncells < 0) {
+    set_error("null pointer or negative size");
+    return CANOE_ERR_ARG;
+  }
+  if (int rc = check_thermo(*th)) return rc;
+  if (opts->warm != 1 && opts->warm != 2) {
+    set_error("the learned saturation adjustment needs opts->warm 1 or 2");
+    return CANOE_ERR_ARG;
+  }
+  MlpView mv = mlp_view(m);
+  return launch_satadj(*th, *opts, d_u, ncells, ncells, nullptr, nullptr, d_t_out, d_iters,
+                       d_stats, (cudaStream_t)stream, &mv, d_guess_out);
 }
 
 int canoe_block_error_word(canoe_block_t b, uint32_t *bits) {

@@ -30,6 +30,10 @@ namespace cb {
 
 enum ColMode { kColFluxOnly = 0, kColStep = 1, kColSolveOnly = 2 };
 
+// threads per pencil: 5 warps cover the nx1 + 1 faces and nx1 + 2 cells of a
+// 128-level column in one pass
+constexpr int kColThreads = 160;
+
 template <int N>
 struct ColRow {
   static constexpr int NN = N * N;
@@ -62,7 +66,7 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
 // FP32 on the perturbation p' from the FP64 hydrostatic face pressure psf;
 // the divergence of psf and the gravity source are added in FP64.
 template <int NY, int RECON, int RS, int N, int MODE, typename R>
-__global__ void __launch_bounds__(128, 3)
+__global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     k_x1col(Geom g, canoe_thermo_t th, const double *__restrict__ w,
             double *__restrict__ du, double *__restrict__ u, double *__restrict__ u1,
             const double *__restrict__ dtp, Stage st, int stage,
@@ -265,30 +269,23 @@ __global__ void __launch_bounds__(128, 3)
     const double dt = wght;
     const double idt = 1. / dt;
     const double area = g.dx2 * g.dx3;
-    // P5a: |A| at faces, J at cells
-    for (int t = tid; t < (nx1 + 1) + (nx1 + 2); t += nth) {
-      if (t <= nx1) {
-        const int il = is - 1 + t;  // face between il and il+1
-        double wl[NV], wr[NV];
+    // P5a: |A| at face t (between cells is-1+t and is+t) and J of cell is-1+t
+    for (int t = tid; t < nx1 + 2; t += nth) {
+      const int ic = is - 1 + t;
+      double wl[NV], wr[NV];
 #pragma unroll
-        for (int n = 0; n < NV; ++n) {
-          wl[n] = wp[n * nc1 + il];
-          wr[n] = wp[n * nc1 + il + 1];
-        }
+      for (int n = 0; n < NV; ++n) wl[n] = wp[n * nc1 + ic];
+      M<N> J;
+      jacobian<N, NY>(J, gm1, wl);
+#pragma unroll
+      for (int e = 0; e < NN; ++e) sJ[t * NN + e] = J.a[e / N][e % N];
+      if (t <= nx1) {
+#pragma unroll
+        for (int n = 0; n < NV; ++n) wr[n] = wp[n * nc1 + ic + 1];
         M<N> A;
         abs_jacobian<N, NY>(A, th, gm1, wl, wr);
 #pragma unroll
         for (int e = 0; e < NN; ++e) sA[t * NN + e] = A.a[e / N][e % N];
-      } else {
-        const int q = t - (nx1 + 1);
-        const int ic = is - 1 + q;
-        double wc[NV];
-#pragma unroll
-        for (int n = 0; n < NV; ++n) wc[n] = wp[n * nc1 + ic];
-        M<N> J;
-        jacobian<N, NY>(J, gm1, wc);
-#pragma unroll
-        for (int e = 0; e < NN; ++e) sJ[q * NN + e] = J.a[e / N][e % N];
       }
     }
     __syncthreads();
@@ -503,7 +500,7 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
   const unsigned nblk = (unsigned)g.nx2 * (unsigned)g.nx3;
   auto go = [&](auto kern) -> int {
     if (int rc = ensure_smem((const void *)kern, smem)) return rc;
-    kern<<<nblk, 128, smem, st>>>(g, th, w, du, u, u1, dtp, s, stage, fout);
+    kern<<<nblk, kColThreads, smem, st>>>(g, th, w, du, u, u1, dtp, s, stage, fout);
     CB_CUDA(cudaGetLastError());
     return 0;
   };

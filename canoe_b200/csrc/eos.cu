@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "block.cuh"
+#include "mlp.cuh"
 
 namespace cb {
 
@@ -207,7 +208,10 @@ __device__ __forceinline__ void sat_eval(const canoe_thermo_t &th, const SatCell
   fp = c.rho * (cvd * cvs + dlat);
 }
 
-// returns iterations; flags bit0 fallback, bit1 not converged
+// returns the number of f evaluations; flags bit0 fallback, bit1 not
+// converged.  Start (o.warm): 0 the unadjusted temperature (cold); 1 the
+// guess; 2 hybrid: cold first, and when that does not converge at once the
+// better of the cold Newton step and the guess.
 template <int NY>
 __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                         double *uc, double t_guess, double &t_out, int &flags) {
@@ -274,11 +278,41 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
   int iters = 0;
   bool fallback = false, converged = false;
   double T = t_cold;
-  if (o.warm && isfinite(t_guess) && t_guess > 1. && t_guess < 1.e4) T = t_guess;
+  const bool guess_ok = isfinite(t_guess) && t_guess > 1. && t_guess < 1.e4;
+  if (o.warm == 1 && guess_ok) T = t_guess;
   double fprev = __longlong_as_double(0x7ff0000000000000LL);
   double f, fp;
   double qn[NY + 1];
-  for (int it = 0; it < o.max_iter; ++it) {
+  int it0 = 0;
+  if (o.warm == 2) {
+    sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+    iters++;
+    const double dT = -f / fp;
+    if (fabs(dT) < o.tol) {
+      T += dT;
+      converged = true;
+      sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+      T -= f / fp;
+      iters++;
+    } else if (guess_ok) {
+      double fg, fpg;
+      sat_eval<NY>(th, c, t_guess, -1, 0, fg, fpg, qn);
+      iters++;
+      if (fabs(fg) < fabs(f)) {
+        T = t_guess - fg / fpg;
+        fprev = fabs(fg);
+      } else {
+        T += dT;
+        fprev = fabs(f);
+      }
+      it0 = 1;
+    } else {
+      T += dT;
+      fprev = fabs(f);
+      it0 = 1;
+    }
+  }
+  for (int it = it0; it < o.max_iter && !converged; ++it) {
     sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
     if (!(fabs(f) < fprev) && it > 0) {
       fallback = true;
@@ -357,29 +391,81 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
   return iters;
 }
 
+// network inputs of a conserved cell: rho, specific internal energy, total
+// of the first and second condensable families
 template <int NY>
+__device__ __forceinline__ void mlp_features(const canoe_thermo_t &th, const double *uc,
+                                             float *x) {
+  using S = Slots<NY>;
+  double rho = uc[0];
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) rho += uc[n];
+  const double ke = 0.5 * (uc[S::IVX] * uc[S::IVX] + uc[S::IVY] * uc[S::IVY] +
+                           uc[S::IVZ] * uc[S::IVZ]) / rho;
+  double fam[2] = {0., 0.};
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    if (v >= th.nvapor) break;
+#pragma unroll
+    for (int n = 1; n <= NY; ++n)
+      if (n == 1 + v || n == th.liq_slot[v] || n == th.ice_slot[v]) fam[v] += uc[n];
+  }
+  x[0] = (float)rho;
+  x[1] = (float)((uc[S::IPR] - ke) / rho);
+  x[2] = (float)(fam[0] / rho);
+  x[3] = (float)(fam[1] / rho);
+}
+
+template <int NY, bool LEARNED>
 __global__ void __launch_bounds__(256)
     k_satadj(canoe_thermo_t th, canoe_satadj_opts_t o, double *__restrict__ u,
              int64_t ncells, int64_t stride, Geom g, int use_geom,
              const double *__restrict__ t_guess, double *__restrict__ t_out,
-             int32_t *__restrict__ iters, unsigned long long *stats) {
+             int32_t *__restrict__ iters, unsigned long long *stats, MlpView mv,
+             double *__restrict__ guess_out) {
   using S = Slots<NY>;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int it = 0, fl = 0;
   bool active = t < ncells;
+  __shared__ float sw1[LEARNED ? kMlpH * kMlpIn : 1], sb1[LEARNED ? kMlpH : 1],
+      sb2[LEARNED ? kMlpH : 1], sw3[LEARNED ? kMlpH : 1];
+  __shared__ __align__(16) __nv_bfloat16 sw2[LEARNED ? kMlpH * kMlpH : 2];
+  if constexpr (LEARNED) {
+    for (int q = threadIdx.x; q < kMlpH * kMlpIn; q += blockDim.x) sw1[q] = mv.p[kMlpOffW1 + q];
+    for (int q = threadIdx.x; q < kMlpH; q += blockDim.x) {
+      sb1[q] = mv.p[kMlpOffB1 + q];
+      sb2[q] = mv.p[kMlpOffB2 + q];
+      sw3[q] = mv.p[kMlpOffW3 + q];
+    }
+    for (int q = threadIdx.x; q < kMlpH * kMlpH; q += blockDim.x) sw2[q] = mv.w2h[q];
+    __syncthreads();
+  }
+  int64_t off = t;
+  double uc[S::NV];
   if (active) {
-    int64_t off = t;
     if (use_geom) {
       const int i = g.is + (int)(t % g.nx1);
       const int64_t r = t / g.nx1;
       const int j = g.js + (int)(r % g.nx2), k = g.ks + (int)(r / g.nx2);
       off = (int64_t)k * g.sk + (int64_t)j * g.nc1 + i;
     }
-    double uc[S::NV];
 #pragma unroll
     for (int n = 0; n < S::NV; ++n) uc[n] = u[n * stride + off];
+  }
+  double tg = t_guess && active ? t_guess[t] : 0.;
+  if constexpr (LEARNED) {
+    // every lane of the warp takes part in the tensor-core inference
+    float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f};
+    if (active) mlp_features<NY>(th, uc, x);
+#pragma unroll
+    for (int q = 0; q < kMlpIn; ++q) x[q] = active ? (x[q] - mv.in_mean[q]) * mv.in_istd[q] : 0.f;
+    const float yn = mlp_warp_infer(x, sw1, sb1, sw2, sb2, sw3, mv.p[kMlpOffB3]);
+    tg = (double)(yn * mv.out_std + mv.out_mean);
+    if (guess_out && active) guess_out[t] = tg;
+  }
+  if (active) {
     double T;
-    it = sat_cell<NY>(th, o, uc, t_guess ? t_guess[t] : 0., T, fl);
+    it = sat_cell<NY>(th, o, uc, tg, T, fl);
 #pragma unroll
     for (int n = 1; n <= NY; ++n) u[n * stride + off] = uc[n];
     if (t_out) t_out[t] = T;
@@ -451,14 +537,21 @@ int launch_dt_finalize(double *d_dt, unsigned long long *acc, double cfl,
 int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o, double *u,
                   int64_t ncells, int64_t stride, const Geom *g, const double *t_guess,
                   double *t_out, int32_t *iters, unsigned long long *stats,
-                  cudaStream_t st) {
+                  cudaStream_t st, const MlpView *mlp, double *guess_out) {
   if (ncells <= 0) return 0;
   Geom gg{};
   if (g) gg = *g;
+  MlpView mv{};
+  if (mlp) mv = *mlp;
   const unsigned nb = (unsigned)((ncells + 255) / 256);
   const int ug = g ? 1 : 0;
-#define CB_SAT(NY) \
-  k_satadj<NY><<<nb, 256, 0, st>>>(th, o, u, ncells, stride, gg, ug, t_guess, t_out, iters, stats)
+#define CB_SAT(NY)                                                                        \
+  if (mlp)                                                                                \
+    k_satadj<NY, true><<<nb, 256, 0, st>>>(th, o, u, ncells, stride, gg, ug, t_guess, t_out, \
+                                           iters, stats, mv, guess_out);                  \
+  else                                                                                    \
+    k_satadj<NY, false><<<nb, 256, 0, st>>>(th, o, u, ncells, stride, gg, ug, t_guess, t_out, \
+                                            iters, stats, mv, guess_out)
   switch (th.ny) {
     case 1: CB_SAT(1); break;
     case 2: CB_SAT(2); break;

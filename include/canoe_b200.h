@@ -92,7 +92,9 @@ typedef struct canoe_thermo {
 typedef struct canoe_satadj_opts {
   double tol;      /* |dT| stopping tolerance [K]                       */
   int32_t max_iter;/* Newton iterations before the bracketing fallback  */
-  int32_t warm;    /* 1: take the initial guess from t_guess[]          */
+  int32_t warm;    /* start: 0 the unadjusted temperature, 1 t_guess[],
+                      2 hybrid: the cold start unless it fails to converge
+                      in one step, then the better of the two           */
 } canoe_satadj_opts_t;
 
 /* One MeshBlock: a Cartesian (or cubed-sphere panel) block. */
@@ -112,6 +114,7 @@ typedef struct canoe_block_config {
 } canoe_block_config_t;
 
 typedef struct canoe_block *canoe_block_t;
+typedef struct canoe_mlp *canoe_mlp_t;
 
 /* ---------------- version / diagnostics ---------------- */
 const char *canoe_version(void);
@@ -146,6 +149,44 @@ int canoe_saturation_adjust(const canoe_thermo_t *th,
                             int64_t ncells, const double *d_t_guess,
                             double *d_t_out, int32_t *d_iters,
                             unsigned long long *d_stats, void *stream);
+
+/* ---------------- learned warm start (no reference counterpart) ---------
+ * A 4 -> 64 -> 64 -> 1 tanh network maps (density, specific internal
+ * energy, total H2O, total NH3) to the converged temperature of the
+ * saturation adjustment.  It only supplies the Newton starting point: the
+ * tolerance, the fallback and therefore the answer are those of the plain
+ * solve.  Parameters are FP32 (layout w1[64*4] b1[64] w2[64*64] b2[64]
+ * w3[64] b3[1], row-major [out][in]); inference uses a BF16 copy of w2 on
+ * the tensor cores with FP32 accumulation. */
+int canoe_mlp_create(uint64_t seed, canoe_mlp_t *out);
+int canoe_mlp_destroy(canoe_mlp_t m);
+int canoe_mlp_nparams(void);
+int canoe_mlp_set_params(canoe_mlp_t m, const float *h_params);
+int canoe_mlp_get_params(canoe_mlp_t m, float *h_params);
+/* inputs are normalised as (x - mean) / std, the output as T = y std + mean */
+int canoe_mlp_set_normalization(canoe_mlp_t m, const float *in_mean, const float *in_std,
+                                float out_mean, float out_std);
+int canoe_mlp_get_normalization(canoe_mlp_t m, float *in_mean, float *in_std,
+                                float *out_mean, float *out_std);
+/* mean-squared error of normalised outputs d_y over n normalised inputs
+ * d_x (n x 4) and its gradient (into d_grad, or the network's own buffer
+ * when NULL); *loss_out (may be NULL) receives the loss (blocking). */
+int canoe_mlp_loss_grad(canoe_mlp_t m, const float *d_x, const float *d_y, int64_t n,
+                        float *d_grad, float *loss_out, void *stream);
+/* one Adam step with the network's own gradient buffer */
+int canoe_mlp_adam_step(canoe_mlp_t m, float lr, float beta1, float beta2, float eps,
+                        void *stream);
+/* normalised forward pass: FP32 CUDA cores (tensor_core = 0) or the BF16
+ * tensor-core path of the warm start (tensor_core = 1) */
+int canoe_mlp_forward(canoe_mlp_t m, const float *d_x, float *d_y, int64_t n, int tensor_core,
+                      void *stream);
+/* canoe_saturation_adjust with the network's guess as the starting point
+ * (opts->warm 1 or 2); d_guess_out (may be NULL) receives the guesses. */
+int canoe_saturation_adjust_learned(const canoe_thermo_t *th,
+                                    const canoe_satadj_opts_t *opts, canoe_mlp_t m,
+                                    double *d_u, int64_t ncells, double *d_t_out,
+                                    int32_t *d_iters, unsigned long long *d_stats,
+                                    double *d_guess_out, void *stream);
 
 /* ---------------- MeshBlock-level entry points ---------------- */
 
@@ -216,6 +257,15 @@ int canoe_block_synchronize(canoe_block_t b);
 /* Hydro::NewBlockTimeStep with canoe patches/21.new_blockdt.patch:20-40;
  * reads back the CFL time step of the current state. */
 int canoe_block_new_dt(canoe_block_t b, double *dt_out);
+
+/* Use the network m (NULL: none) for the saturation adjustment of every
+ * following step, in the hybrid start mode.  The network must outlive its
+ * use by the block.  No reference counterpart. */
+int canoe_block_set_mlp(canoe_block_t b, canoe_mlp_t m);
+
+/* read and clear the block's saturation-adjustment counters {cells,
+ * evaluations of f, fallbacks, not converged} accumulated by its steps */
+int canoe_block_satadj_stats(canoe_block_t b, unsigned long long *h_stats);
 
 /* read and clear the block's device error word (canoe_errbit bits) */
 int canoe_block_error_word(canoe_block_t b, uint32_t *bits);

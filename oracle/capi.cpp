@@ -140,6 +140,7 @@ int oracle_prim_to_cons(const canoe_thermo_t *th, const double *w, double *u,
 int oracle_satadj(const canoe_thermo_t *th, const canoe_satadj_opts_t *o,
                   double *u, int64_t n, const double *t_guess, double *t_out,
                   int32_t *iters, int32_t *flags) {
+  // o->warm: 0 cold, 1 start at t_guess, 2 hybrid (see satadj_cell)
 #pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < n; ++c) {
     oracle::SatResult r =

@@ -152,11 +152,15 @@ def prim_to_cons(th, w):
     return u
 
 
-def satadj(th, u, tol=1e-8, max_iter=30, t_guess=None):
-    """Saturation adjustment of cells u (NV, n) in place; returns T, iters, flags."""
+def satadj(th, u, tol=1e-8, max_iter=30, t_guess=None, mode=None):
+    """Saturation adjustment of cells u (NV, n) in place; returns T, iters
+    (evaluations of f), flags.  mode: 0 cold, 1 start at t_guess, 2 hybrid
+    (default 1 when t_guess is given, else 0)."""
     assert u.flags.c_contiguous and u.dtype == np.float64
     n = u.shape[1]
-    o = SatOpts(tol, max_iter, 1 if t_guess is not None else 0)
+    if mode is None:
+        mode = 1 if t_guess is not None else 0
+    o = SatOpts(tol, max_iter, mode)
     t = np.zeros(n)
     it = np.zeros(n, dtype=np.int32)
     fl = np.zeros(n, dtype=np.int32)

@@ -142,10 +142,42 @@ SatResult satadj_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
 
   SatResult r{t_cold, 0, false, false};
   double T = t_cold;
-  if (o.warm && std::isfinite(t_guess) && t_guess > 1. && t_guess < 1.e4) T = t_guess;
+  // start (o.warm): 0 cold, 1 the guess, 2 hybrid: cold first and, when that
+  // does not converge at once, the better of the cold Newton step and the
+  // guess.  iters counts evaluations of f.
+  const bool guess_ok = std::isfinite(t_guess) && t_guess > 1. && t_guess < 1.e4;
+  if (o.warm == 1 && guess_ok) T = t_guess;
   double fprev = std::numeric_limits<double>::infinity();
   Eval e;
-  for (int it = 0; it < o.max_iter; ++it) {
+  int it0 = 0;
+  if (o.warm == 2) {
+    e = evaluate(th, c, T);
+    r.iters++;
+    double dT = -e.f / e.fp;
+    if (std::fabs(dT) < o.tol) {
+      T += dT;
+      r.converged = true;
+      e = evaluate(th, c, T);
+      T -= e.f / e.fp;
+      r.iters++;
+    } else if (guess_ok) {
+      Eval eg = evaluate(th, c, t_guess);
+      r.iters++;
+      if (std::fabs(eg.f) < std::fabs(e.f)) {
+        T = t_guess - eg.f / eg.fp;
+        fprev = std::fabs(eg.f);
+      } else {
+        T += dT;
+        fprev = std::fabs(e.f);
+      }
+      it0 = 1;
+    } else {
+      T += dT;
+      fprev = std::fabs(e.f);
+      it0 = 1;
+    }
+  }
+  for (int it = it0; it < o.max_iter && !r.converged; ++it) {
     e = evaluate(th, c, T);
     if (!(std::fabs(e.f) < fprev) && it > 0) {
       r.fallback = true;
