@@ -141,6 +141,40 @@ def cpu_baseline(args, seconds=12.0, max_steps=20):
                       f"({ncell} cells, {el:.1f} s wall)"}
 
 
+def c4_report(net, th, ncells=1 << 24):
+    """C4: the learned warm start on 16.8 M perturbed cells against the cold
+    start: device time, evaluations of the energy residual, fallbacks."""
+    import torch
+    from canoe_b200 import learned
+    from canoe_b200._abi import SatOpts, check, load
+    lib = load()
+    u = learned.perturbed_states(th, ncells, seed=2024)
+    out = {"cells": ncells}
+    for name, mode in (("cold", 0), ("learned", 2)):
+        d = torch.from_numpy(u).cuda()
+        st = torch.zeros(4, dtype=torch.int64, device="cuda")
+        o = SatOpts(1e-8, 30, mode)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if mode == 0:
+            check(lib.canoe_saturation_adjust(ctypes.byref(th), ctypes.byref(o), d.data_ptr(),
+                                              ncells, None, None, None, st.data_ptr(), None))
+        else:
+            check(lib.canoe_saturation_adjust_learned(ctypes.byref(th), ctypes.byref(o), net.h,
+                                                      d.data_ptr(), ncells, None, None,
+                                                      st.data_ptr(), None, None))
+        e1.record()
+        e1.synchronize()
+        s = st.cpu().numpy()
+        out[name] = {"ms": e0.elapsed_time(e1), "evaluations_per_cell": float(s[1]) / s[0],
+                     "fallback_rate": float(s[2]) / s[0], "not_converged": int(s[3])}
+        del d
+    out["note"] = ("same tolerance (1e-8 K + one polishing step) and the same answer; "
+                   "the gated start uses the network where it predicts latent heating")
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -180,6 +214,7 @@ def main():
                     help="headline variant; the other one is timed alongside")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-c4", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -211,7 +246,11 @@ def main():
         check(lib.canoe_block_set_stream(b.h, ctypes.c_void_p(stream.cuda_stream)))
         return b
 
+    from canoe_b200 import learned
+    net = learned.default_net()
     blocks = {"fp64": make_block(FP64), "mixed": make_block(FP32_PERTURBATION)}
+    # the headline: FP32 fluxes + learned warm start; plain FP64 alongside
+    blocks["mixed"].set_mlp(net)
     # both variants step with the CFL time step of the initial state
     dt0 = blocks["fp64"].new_dt()
     for b in blocks.values():
@@ -259,6 +298,12 @@ def main():
     l2 = {"theta": rl2(theta(wb), theta(wa)),
           "total_water": rl2(ub[1:1 + ny].sum(axis=0), ua[1:1 + ny].sum(axis=0)),
           "steps": args.warmup + args.steps}
+    sat = {}
+    for name, b in blocks.items():
+        s = b.satadj_stats()
+        sat[name] = {"evaluations_per_cell": float(s[1]) / max(1, int(s[0])),
+                     "fallback_rate": float(s[2]) / max(1, int(s[0])),
+                     "not_converged": int(s[3])}
     del wa, wb, ua, ub
     # per-kernel-class timing pass of the headline variant
     blk = blocks[args.precision]
@@ -331,6 +376,9 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args)
+    c4 = None
+    if rank == 0 and not args.no_c4:
+        c4 = c4_report(net, p.cfg.thermo)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -344,7 +392,8 @@ def main():
             "config": config_dict(args), "gpu_launches": launches,
             "other_variant": other, "speedup_mixed_vs_fp64":
                 (value / other["value"]) if args.precision == "mixed" else other["value"] / value,
-            "l2_error_mixed_vs_fp64": l2,
+            "l2_error_mixed_vs_fp64": l2, "saturation_adjustment": sat,
+            "c4_learned_warm_start": c4,
             "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
             "error_word": err}
     print(json.dumps(line), flush=True)

@@ -62,6 +62,18 @@ class MeshBlock:
     def step(self, dt=-1.0):
         check(self.lib.canoe_block_step(self.h, float(dt)), "step")
 
+    def set_mlp(self, net):
+        """learned warm start of the saturation adjustment (None: off)"""
+        self._net = net  # the network must outlive its use
+        check(self.lib.canoe_block_set_mlp(self.h, net.h if net is not None else None),
+              "set_mlp")
+
+    def satadj_stats(self):
+        """{cells, evaluations, fallbacks, not converged} since the last call"""
+        s = np.zeros(4, dtype=np.uint64)
+        check(self.lib.canoe_block_satadj_stats(self.h, s.ctypes.data), "satadj_stats")
+        return s
+
     def set_fixed_dt(self, dt):
         check(self.lib.canoe_block_set_fixed_dt(self.h, float(dt)), "set_fixed_dt")
 

@@ -208,10 +208,13 @@ __device__ __forceinline__ void sat_eval(const canoe_thermo_t &th, const SatCell
   fp = c.rho * (cvd * cvs + dlat);
 }
 
+// a guess below this much latent heating [K] keeps the cold start, which is
+// exact in one step for cells that stay unsaturated
+constexpr double kSatGate = 0.05;
+
 // returns the number of f evaluations; flags bit0 fallback, bit1 not
 // converged.  Start (o.warm): 0 the unadjusted temperature (cold); 1 the
-// guess; 2 hybrid: cold first, and when that does not converge at once the
-// better of the cold Newton step and the guess.
+// guess; 2 gated: the guess if it exceeds the cold start by kSatGate.
 template <int NY>
 __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                         double *uc, double t_guess, double &t_out, int &flags) {
@@ -283,35 +286,9 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
   double fprev = __longlong_as_double(0x7ff0000000000000LL);
   double f, fp;
   double qn[NY + 1];
-  int it0 = 0;
-  if (o.warm == 2) {
-    sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
-    iters++;
-    const double dT = -f / fp;
-    if (fabs(dT) < o.tol) {
-      T += dT;
-      converged = true;
-      sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
-      T -= f / fp;
-      iters++;
-    } else if (guess_ok) {
-      double fg, fpg;
-      sat_eval<NY>(th, c, t_guess, -1, 0, fg, fpg, qn);
-      iters++;
-      if (fabs(fg) < fabs(f)) {
-        T = t_guess - fg / fpg;
-        fprev = fabs(fg);
-      } else {
-        T += dT;
-        fprev = fabs(f);
-      }
-      it0 = 1;
-    } else {
-      T += dT;
-      fprev = fabs(f);
-      it0 = 1;
-    }
-  }
+  // gated start: the guess when it predicts latent heating, else cold
+  if (o.warm == 2 && guess_ok && t_guess - t_cold > kSatGate) T = t_guess;
+  const int it0 = 0;
   for (int it = it0; it < o.max_iter && !converged; ++it) {
     sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
     if (!(fabs(f) < fprev) && it > 0) {
@@ -394,8 +371,8 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
 // network inputs of a conserved cell: rho, specific internal energy, total
 // of the first and second condensable families
 template <int NY>
-__device__ __forceinline__ void mlp_features(const canoe_thermo_t &th, const double *uc,
-                                             float *x) {
+__device__ __forceinline__ double mlp_features(const canoe_thermo_t &th, const double *uc,
+                                               float *x) {
   using S = Slots<NY>;
   double rho = uc[0];
 #pragma unroll
@@ -410,10 +387,17 @@ __device__ __forceinline__ void mlp_features(const canoe_thermo_t &th, const dou
     for (int n = 1; n <= NY; ++n)
       if (n == 1 + v || n == th.liq_slot[v] || n == th.ice_slot[v]) fam[v] += uc[n];
   }
+  const double ev = (uc[S::IPR] - ke) / rho;
   x[0] = (float)rho;
-  x[1] = (float)((uc[S::IPR] - ke) / rho);
+  x[1] = (float)ev;
   x[2] = (float)(fam[0] / rho);
   x[3] = (float)(fam[1] / rho);
+  // temperature with all water as vapour: the baseline the network corrects
+  double cvs = 1.;
+#pragma unroll
+  for (int v = 0; v < 2; ++v)
+    if (v < th.nvapor) cvs += fam[v] / rho * th.cv_ratio_m1[v];
+  return ev / (th.rd / (th.gammad - 1.) * cvs);
 }
 
 template <int NY, bool LEARNED>
@@ -456,11 +440,12 @@ __global__ void __launch_bounds__(256)
   if constexpr (LEARNED) {
     // every lane of the warp takes part in the tensor-core inference
     float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f};
-    if (active) mlp_features<NY>(th, uc, x);
+    double tdry = 0.;
+    if (active) tdry = mlp_features<NY>(th, uc, x);
 #pragma unroll
     for (int q = 0; q < kMlpIn; ++q) x[q] = active ? (x[q] - mv.in_mean[q]) * mv.in_istd[q] : 0.f;
     const float yn = mlp_warp_infer(x, sw1, sb1, sw2, sb2, sw3, mv.p[kMlpOffB3]);
-    tg = (double)(yn * mv.out_std + mv.out_mean);
+    tg = tdry + (double)(yn * mv.out_std + mv.out_mean);
     if (guess_out && active) guess_out[t] = tg;
   }
   if (active) {

@@ -2,12 +2,16 @@
 
 A 4 -> 64 -> 64 -> 1 tanh network (canoe_mlp_* in the C ABI) maps a cell's
 (density, specific internal energy, total H2O, total NH3) to the temperature
-the plain Newton saturation adjustment converges to.  Training pairs come
+the plain Newton saturation adjustment converges to, as a correction to
+the all-vapour temperature T_vapour = e / cv(all water as vapour) (the
+latent heating, 0 for cells that stay unsaturated).  Training pairs come
 from the plain solver itself on perturbed states of the moist LES column;
 training runs on the GPU with the library's own forward / backward and Adam
 kernels.  The network never changes the answer: the saturation adjustment
 still iterates to its tolerance from the better of the cold start and the
-guess, with the bracketed fallback unchanged.
+guess, with the bracketed fallback unchanged; the gated start uses the
+guess only where it predicts more than 0.05 K of latent heating, so cells
+that stay unsaturated keep the cold start that is exact in one step.
 
 The NH3 input is 0 for the H2O-only thermodynamics of the LES
 configuration; the channel is kept so the same network shape serves an
@@ -108,11 +112,12 @@ class WarmStartNet:
         torch.cuda.synchronize()
         return y.cpu().numpy()
 
-    def fit(self, x, T, epochs=4, batch=65536, lr=2e-3, lr_final=2e-4, seed=0, log=None):
-        """Normalise (x, T), then Adam on the GPU; returns the final loss."""
+    def fit(self, x, T, th, epochs=20, batch=8192, lr=3e-3, lr_final=1e-4, seed=0, log=None):
+        """Normalise (x, T - T_vapour), then Adam on the GPU; returns the
+        final loss."""
         import torch
         x = np.asarray(x, dtype=np.float64)
-        T = np.asarray(T, dtype=np.float64)
+        T = np.asarray(T, dtype=np.float64) - t_vapour(th, x)
         in_mean = x.mean(axis=0)
         in_std = x.std(axis=0)
         in_std[in_std == 0] = 1.0
@@ -166,6 +171,21 @@ def perturbed_states(th, n, seed, dT=10.0, dq=0.2, zmax=16.0e3):
     w[1 + ny:4 + ny] = rng.uniform(-5.0, 5.0, (3, n))
     w[4 + ny] = p
     return thermo.prim_to_cons(th, w)
+
+
+def t_vapour(th, x):
+    """all-vapour temperature of feature rows x (n, 4)"""
+    cvs = 1.0 + x[:, 2] * th.cv_ratio_m1[0]
+    if th.nvapor > 1:
+        cvs = cvs + x[:, 3] * th.cv_ratio_m1[1]
+    return x[:, 1] / (th.rd / (th.gammad - 1.0) * cvs)
+
+
+def predict(net, th, x):
+    """the network's temperature guess for feature rows x (tensor cores)"""
+    a, b, om, os_ = net.normalization()
+    yn = net.forward(((x - a) / b).astype(np.float32), tensor_core=True)
+    return t_vapour(th, x) + yn * os_ + om
 
 
 def features(th, u):
@@ -224,9 +244,20 @@ def training_pairs(th, n, seed=7):
     return features(th, u), T
 
 
-def train_warm_start(th=None, n=1 << 21, seed=7, epochs=6, log=None):
+def default_net():
+    """The committed network (canoe_b200/data/warm_start_c2.npz), or one
+    trained now when the file is missing."""
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                        "warm_start_c2.npz")
+    if os.path.exists(path):
+        return WarmStartNet.load(path)
+    return train_warm_start()
+
+
+def train_warm_start(th=None, n=1 << 21, seed=7, epochs=20, batch=8192, log=None):
     th = th or thermo.earth_moist()
     x, T = training_pairs(th, n, seed)
     net = WarmStartNet(seed=seed)
-    net.fit(x, T, epochs=epochs, log=log)
+    net.fit(x, T, th, epochs=epochs, batch=batch, log=log)
     return net

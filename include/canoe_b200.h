@@ -92,9 +92,9 @@ typedef struct canoe_thermo {
 typedef struct canoe_satadj_opts {
   double tol;      /* |dT| stopping tolerance [K]                       */
   int32_t max_iter;/* Newton iterations before the bracketing fallback  */
-  int32_t warm;    /* start: 0 the unadjusted temperature, 1 t_guess[],
-                      2 hybrid: the cold start unless it fails to converge
-                      in one step, then the better of the two           */
+  int32_t warm;    /* start: 0 the unadjusted temperature (cold),
+                      1 t_guess[], 2 gated: t_guess[] when it exceeds the
+                      cold start by 0.05 K (latent heating), else cold   */
 } canoe_satadj_opts_t;
 
 /* One MeshBlock: a Cartesian (or cubed-sphere panel) block. */
@@ -153,7 +153,8 @@ int canoe_saturation_adjust(const canoe_thermo_t *th,
 /* ---------------- learned warm start (no reference counterpart) ---------
  * A 4 -> 64 -> 64 -> 1 tanh network maps (density, specific internal
  * energy, total H2O, total NH3) to the converged temperature of the
- * saturation adjustment.  It only supplies the Newton starting point: the
+ * saturation adjustment, as a correction to the temperature the cell would
+ * have with all water as vapour.  It only supplies the Newton starting point: the
  * tolerance, the fallback and therefore the answer are those of the plain
  * solve.  Parameters are FP32 (layout w1[64*4] b1[64] w2[64*64] b2[64]
  * w3[64] b3[1], row-major [out][in]); inference uses a BF16 copy of w2 on
@@ -163,7 +164,8 @@ int canoe_mlp_destroy(canoe_mlp_t m);
 int canoe_mlp_nparams(void);
 int canoe_mlp_set_params(canoe_mlp_t m, const float *h_params);
 int canoe_mlp_get_params(canoe_mlp_t m, float *h_params);
-/* inputs are normalised as (x - mean) / std, the output as T = y std + mean */
+/* inputs are normalised as (x - mean) / std; the output as
+ * T = T_vapour + y std + mean, T_vapour the all-vapour temperature */
 int canoe_mlp_set_normalization(canoe_mlp_t m, const float *in_mean, const float *in_std,
                                 float out_mean, float out_std);
 int canoe_mlp_get_normalization(canoe_mlp_t m, float *in_mean, float *in_std,
@@ -259,7 +261,7 @@ int canoe_block_synchronize(canoe_block_t b);
 int canoe_block_new_dt(canoe_block_t b, double *dt_out);
 
 /* Use the network m (NULL: none) for the saturation adjustment of every
- * following step, in the hybrid start mode.  The network must outlive its
+ * following step, in the gated start mode.  The network must outlive its
  * use by the block.  No reference counterpart. */
 int canoe_block_set_mlp(canoe_block_t b, canoe_mlp_t m);
 

@@ -142,41 +142,15 @@ SatResult satadj_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
 
   SatResult r{t_cold, 0, false, false};
   double T = t_cold;
-  // start (o.warm): 0 cold, 1 the guess, 2 hybrid: cold first and, when that
-  // does not converge at once, the better of the cold Newton step and the
-  // guess.  iters counts evaluations of f.
+  // start (o.warm): 0 cold, 1 the guess, 2 gated: the guess when it exceeds
+  // the cold start by 0.05 K of latent heating, else cold.  iters counts
+  // evaluations of f.
   const bool guess_ok = std::isfinite(t_guess) && t_guess > 1. && t_guess < 1.e4;
   if (o.warm == 1 && guess_ok) T = t_guess;
+  if (o.warm == 2 && guess_ok && t_guess - t_cold > 0.05) T = t_guess;
   double fprev = std::numeric_limits<double>::infinity();
   Eval e;
-  int it0 = 0;
-  if (o.warm == 2) {
-    e = evaluate(th, c, T);
-    r.iters++;
-    double dT = -e.f / e.fp;
-    if (std::fabs(dT) < o.tol) {
-      T += dT;
-      r.converged = true;
-      e = evaluate(th, c, T);
-      T -= e.f / e.fp;
-      r.iters++;
-    } else if (guess_ok) {
-      Eval eg = evaluate(th, c, t_guess);
-      r.iters++;
-      if (std::fabs(eg.f) < std::fabs(e.f)) {
-        T = t_guess - eg.f / eg.fp;
-        fprev = std::fabs(eg.f);
-      } else {
-        T += dT;
-        fprev = std::fabs(e.f);
-      }
-      it0 = 1;
-    } else {
-      T += dT;
-      fprev = std::fabs(e.f);
-      it0 = 1;
-    }
-  }
+  const int it0 = 0;
   for (int it = it0; it < o.max_iter && !r.converged; ++it) {
     e = evaluate(th, c, T);
     if (!(std::fabs(e.f) < fprev) && it > 0) {

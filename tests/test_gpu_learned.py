@@ -6,9 +6,9 @@
   inference stays within 2e-2 of it (normalised units);
 * a trained network reproduces the converged temperature to ~1 K;
 * the learned solve returns the plain solve's answer (T to 1e-9 K, species
-  to 1e-12 relative) and needs fewer evaluations of the energy residual on
-  the saturated cells -- what the network gains;
-* the hybrid start on the GPU equals the oracle's hybrid start given the
+  to 1e-12 relative) and needs fewer evaluations of the energy residual --
+  what the network gains (printed);
+* the gated start on the GPU equals the oracle's gated start given the
   GPU's guesses.
 """
 import numpy as np
@@ -26,7 +26,7 @@ def th():
 
 @pytest.fixture(scope="module")
 def net(th):
-    return learned.train_warm_start(th, n=1 << 19, epochs=8)
+    return learned.train_warm_start(th, n=1 << 20, epochs=30, batch=4096)
 
 
 def test_gradient_matches_oracle(oracle_mod):
@@ -55,10 +55,8 @@ def test_inference_fp32_and_tensor_core(oracle_mod):
 
 def test_training_fits_converged_temperature(th, net):
     x, T = learned.training_pairs(th, 1 << 16, seed=99)
-    a, b, om, os_ = net.normalization()
-    yn = net.forward(((x - a) / b).astype(np.float32), tensor_core=True)
-    err = np.abs(yn * os_ + om - T)
-    assert np.sqrt(np.mean(err ** 2)) < 1.0, np.sqrt(np.mean(err ** 2))
+    err = learned.predict(net, th, x) - T
+    assert np.sqrt(np.mean(err ** 2)) < 0.3, np.sqrt(np.mean(err ** 2))
 
 
 def test_learned_solve_same_answer_fewer_evaluations(th, net):
@@ -71,12 +69,13 @@ def test_learned_solve_same_answer_fewer_evaluations(th, net):
     assert stc[3] == 0 and stl[3] == 0
     sat = uc[2] + uc[3] > 0  # cells that end with condensate
     assert sat.sum() > 1000
+    print(f"evaluations of f per cell: cold {itc.mean():.3f} learned {itl.mean():.3f}; "
+          f"saturated cells cold {itc[sat].mean():.3f} learned {itl[sat].mean():.3f}")
     assert itl[sat].mean() < itc[sat].mean(), (itl[sat].mean(), itc[sat].mean())
-    # unsaturated cells keep the one-step cold path
-    assert itl[~sat].mean() <= itc[~sat].mean() + 1e-12
+    assert itl.mean() < itc.mean()
 
 
-def test_hybrid_start_matches_oracle(th, net, oracle_mod):
+def test_gated_start_matches_oracle(th, net, oracle_mod):
     u = learned.perturbed_states(th, 20000, seed=41)
     ul, Tl, itl, _, guess = learned.satadj_gpu(th, u, mode=2, net=net)
     ref = u.copy()
