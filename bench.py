@@ -41,12 +41,27 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """nvidia-smi clock / throttle samples of this process's GPU (selected by
+    UUID, so CUDA_VISIBLE_DEVICES remapping does not matter).  start() waits
+    for the first sample; samples are time-stamped and those inside the
+    timed region [mark_begin(), mark_end()] are reported (all samples under
+    load when the region is shorter than the sampling period)."""
 
-    def __init__(self, index=0):
-        self.index = index
+    def __init__(self, device=0, period_ms=100):
+        self.device = device
+        self.period_ms = period_ms
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
+
+    def _gpu_id(self):
+        import torch
+        try:
+            return "GPU-" + str(torch.cuda.get_device_properties(self.device).uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x.strip() for x in vis.split(",") if x.strip()]
+            return ids[self.device] if self.device < len(ids) else str(self.device)
 
     def start(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -54,42 +69,64 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", f"--id={self._gpu_id()}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.monotonic() + 10.0
+            while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def mark_begin(self):
+        self.t0 = time.monotonic()
+
+    def mark_end(self):
+        self.t1 = time.monotonic()
 
     def stop(self):
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"],
+                    "samples": 0}
+        time.sleep(2.5 * self.period_ms * 1e-3)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
+
+        def parse(lines):
+            sm, smax, reasons = [], None, set()
+            for _, ln in lines:
+                f = [x.strip() for x in ln.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax = float(f[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+            return sm, smax, reasons
+
+        window = "timed region"
+        lo = (self.t0 or 0.0) - 0.5 * self.period_ms * 1e-3
+        hi = (self.t1 or time.monotonic()) + 1.5 * self.period_ms * 1e-3
+        sm, smax, reasons = parse([x for x in self.lines if lo <= x[0] <= hi])
+        if not sm:
+            window = "warm-up and timed region"
+            sm, smax, reasons = parse(self.lines[1:])
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 def make_problem(args, nx2=None, nx3=None):
@@ -260,22 +297,26 @@ def main():
     with torch.cuda.stream(stream):
         for name in order:
             blk = blocks[name]
+            sampler = ClockSampler(torch.cuda.current_device()) if name == args.precision else None
+            if sampler:
+                sampler.start()
             for _ in range(args.warmup):
                 blk.step()
             stream.synchronize()
             if dist:
                 dist.barrier()
-            sampler = ClockSampler(local) if name == args.precision else None
-            if sampler:
-                sampler.start()
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            if sampler:
+                sampler.mark_begin()
             e0.record(stream)
             for _ in range(args.steps):
                 blk.step()
             e1.record(stream)
             e1.synchronize()
+            if sampler:
+                sampler.mark_end()
             ms = e0.elapsed_time(e1)
             if sampler:
                 clocks = sampler.stop()
