@@ -76,6 +76,8 @@ SIGNATURES = [
     ("canoe_block_set_fixed_dt", c_int, [c_void_p, c_double]),
     ("canoe_block_step_profile", c_int, [c_void_p, c_double, POINTER(ctypes.c_float), c_int]),
     ("canoe_block_step", c_int, [c_void_p, c_double]),
+    ("canoe_block_step_noalloc", c_int, [POINTER(BlockConfig), c_void_p, c_void_p, c_void_p,
+                                         c_double, c_void_p]),
     ("canoe_block_new_dt", c_int, [c_void_p, POINTER(c_double)]),
     ("canoe_block_error_word", c_int, [c_void_p, POINTER(c_uint32)]),
     ("canoe_block_set_mlp", c_int, [c_void_p, c_void_p]),

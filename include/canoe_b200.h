@@ -234,6 +234,32 @@ int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt);
  * patches/21.new_blockdt.patch) computed on the device. */
 int canoe_block_step(canoe_block_t b, double dt);
 
+/* One time step like canoe_block_step(b, dt) that allocates nothing, for
+ * callers that cannot let a library allocate device memory while they run
+ * (a host model whose memory pool holds the GPU's memory, where a cudaMalloc
+ * would fail or synchronize the device inside its own time step).  No
+ * counterpart in the reference (its MeshBlock owns its arrays,
+ * src/interface/hydro.hpp:54-67).
+ *   cfg   block configuration as for canoe_block_create
+ *   d_u   device conserved state (NV, nc3, nc2, nc1), ghosts included:
+ *         read, advanced by dt in place
+ *   d_w   device buffer of the same shape: receives the primitive state
+ *         (with ghosts) of the advanced u
+ *   d_err optional device word, cleared, then set to canoe_errbit bits;
+ *         NULL keeps the bits in the library's scratch
+ *   dt    time step (> 0); the pressure profile of the FP32 flux path is
+ *         the level mean of the state on entry
+ * The step's other arrays (du, u1, geometry, dt) live in one fixed device
+ * array of 16 MiB (2 Mi doubles) per device, which must hold
+ * 2 NV nc3 nc2 nc1 + 4 nc1 + 8 doubles: larger blocks return CANOE_ERR_ARG.
+ * The first call on a device looks up that array's address; make it before
+ * any stream capture begins.  All calls on a device share the array, so
+ * calls that overlap in time (other streams or threads) race and corrupt
+ * each other's results: order them on one stream.  The saturation
+ * adjustment (cfg->satadj) uses the cold start. */
+int canoe_block_step_noalloc(const canoe_block_config_t *cfg, double *d_u, double *d_w,
+                             uint32_t *d_err, double dt, void *stream);
+
 /* Capture one step (all RK stages, device dt) as a CUDA graph on first use and
  * replay it for every canoe_block_step(b, dt <= 0) call.  No reference
  * counterpart: the reference drives the task list from the host per stage
