@@ -26,6 +26,11 @@ struct Geom {
   // horizontally uniform reference pressure per x1 level (nc1): the FP32
   // flux path works on p' = p - pref so that p ~ 1e5 never enters FP32
   const double *pref;
+  // device error word (canoe_errbit) for kernels that report on their own
+  uint32_t *err;
+  // set per launch: 1 when the pencil rows may be moved by bulk copies
+  // (16-byte aligned arrays, nc1 even)
+  int bulk;
 };
 
 // RK3 (SSPRK(3,3), Shu & Osher 1988) register weights per stage:

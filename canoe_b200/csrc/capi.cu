@@ -386,6 +386,7 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
   g.x1v = b->d_x1v;
   g.dx1f = b->d_dx1f;
   g.pref = b->d_pref;
+  g.err = b->d_err;
   *out = b;
   return 0;
 }

@@ -25,6 +25,7 @@
 #pragma once
 
 #include "blockmat.cuh"
+#include "bulk.cuh"
 
 namespace cb {
 
@@ -44,27 +45,41 @@ struct ColRow {
 
 // shared-memory plan (doubles) of one pencil
 struct ColSmem {
-  int wp, dc, uni, total;
+  int wp, dc, uni, stg, mbar, total;
 };
+
+__host__ __device__ inline int even_up(int x) { return (x + 1) & ~1; }
 
 __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl) {
   ColSmem s;
   s.wp = 0;                  // [NV][nc1] pristine pencil
-  s.dc = nv * nc1;           // [NV][nx1] du of the column
-  s.uni = s.dc + nv * nx1;   // union region
+  s.dc = nv * nc1;           // [NV][nc1] du of the column (interior at is)
+  s.uni = even_up(2 * nv * nc1);  // union region
   const int flux = 3 * nv * nc1 + 3 * nc1 + 1;
   int solve = 0;
+  s.stg = 0;
   if (n_impl) {
     const int nn = n_impl * n_impl;
-    solve = nx1 * ((3 * nn + n_impl) | 1) + (nx1 + 1) * nn + (nx1 + 2) * nn;
+    const int rows = even_up(nx1 * ((3 * nn + n_impl) | 1));
+    // |A| and J, later reused as the staging area of u and u1
+    const int aj = (nx1 + 1) * nn + (nx1 + 2) * nn;
+    const int st = 2 * nv * nc1;
+    s.stg = s.uni + rows;
+    solve = rows + (aj > st ? aj : st);
   }
-  s.total = s.uni + (flux > solve ? flux : solve);
+  s.mbar = s.uni + even_up(flux > solve ? flux : solve);
+  s.total = s.mbar + 4;  // 3 mbarriers, 8 bytes each
   return s;
 }
 
 // R = double: the FP64 path.  R = float: reconstruction and Riemann fluxes in
 // FP32 on the perturbation p' from the FP64 hydrostatic face pressure psf;
 // the divergence of psf and the gravity source are added in FP64.
+//
+// Latency hiding inside the CTA: the pencil rows of w and du arrive by bulk
+// copies issued at entry; u and u1 are fetched into the dead |A| / J area
+// while the cyclic reduction runs; the serial hydrostatic scan (one lane of
+// warp 0) overlaps the reconstruction of the variables it does not touch.
 template <int NY, int RECON, int RS, int N, int MODE, typename R>
 __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     k_x1col(Geom g, canoe_thermo_t th, const double *__restrict__ w,
@@ -79,17 +94,52 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
   double *wp = sm + L.wp;
   double *dc = sm + L.dc;
   double *un = sm + L.uni;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + L.mbar);
 
   const int j = g.js + (int)(blockIdx.x % (unsigned)g.nx2);
   const int k = g.ks + (int)(blockIdx.x / (unsigned)g.nx2);
   const int64_t base = (int64_t)k * g.sk + (int64_t)j * nc1;
   const int tid = threadIdx.x, nth = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31;
   const double grav = th.grav;
   const double wght = st.beta * dtp[0];
+  const bool bulk = g.bulk != 0;
+  constexpr bool NEED_DU = MODE == kColSolveOnly || MODE == kColStep;
+  const bool load_du = NEED_DU && (MODE == kColSolveOnly || g.f2);
+  const uint32_t row_bytes = (uint32_t)nc1 * 8u;
 
-  // P0: stage the pencil
-  for (int n = 0; n < NV; ++n)
-    for (int i = tid; i < nc1; i += nth) wp[n * nc1 + i] = w[n * g.sv + base + i];
+  // a wait that gave up: report, give the copies still in flight on
+  // mbarriers q0 .. q1-1 a second bounded wait, leave
+  auto bail = [&](int q0, int q1) {
+    if (tid == 0 && g.err) atomicOr(g.err, (uint32_t)CANOE_EBIT_TIMEOUT);
+    for (int q = q0; q < q1; ++q) mbar_wait(mbar + q, 0);
+  };
+
+  // P0: stage the pencil (and du)
+  if (bulk) {
+    if (tid == 0) {
+      for (int q = 0; q < 3; ++q) mbar_init(mbar + q, 1);
+      fence_mbar_init();
+      mbar_expect_tx(mbar, NV * row_bytes);
+      for (int n = 0; n < NV; ++n) bulk_g2s(wp + n * nc1, w + n * g.sv + base, row_bytes, mbar);
+      if (load_du) {
+        mbar_expect_tx(mbar + 1, NV * row_bytes);
+        for (int n = 0; n < NV; ++n)
+          bulk_g2s(dc + n * nc1, du + n * g.sv + base, row_bytes, mbar + 1);
+      }
+    }
+    __syncthreads();
+    if (!__syncthreads_and(mbar_wait(mbar, 0))) {
+      bail(0, load_du ? 2 : 1);
+      return;
+    }
+  } else {
+    for (int n = 0; n < NV; ++n)
+      for (int i = tid; i < nc1; i += nth) wp[n * nc1 + i] = w[n * g.sv + base + i];
+    if (load_du)
+      for (int n = 0; n < NV; ++n)
+        for (int i = is + tid; i <= ie; i += nth) dc[n * nc1 + i] = du[n * g.sv + base + i];
+  }
 
   constexpr bool PERT = sizeof(R) == 4;
   if constexpr (MODE != kColSolveOnly) {
@@ -108,32 +158,65 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         if (n == S::IPR) v -= pcst;
         q[n * nc1 + i] = R(v);
       }
-    // P1
+    __syncthreads();
+    // P2 for variable n over the cells is-1 .. ie+1, items t0, t0+dt, ...
+    const int ncell = nx1 + 2;
+    auto recon = [&](int n, int c) {
+      const R *qn = q + n * nc1;
+      R wl_, wr_;
+      if constexpr (RECON == CANOE_RECON_PPM)
+        ppm_cell(qn[c - 2], qn[c - 1], qn[c], qn[c + 1], qn[c + 2], wl_, wr_);
+      else
+        plm_cell_nu(qn[c - 1], qn[c], qn[c + 1], R(g.x1v[c - 1]), R(g.x1v[c]),
+                    R(g.x1v[c + 1]), R(g.x1f[c]), R(g.x1f[c + 1]), wl_, wr_);
+      WL[n * nc1 + c] = wl_;
+      WR[n * nc1 + c] = wr_;
+    };
+    // P1 (the scan) overlapped with P2 of the variables other than rho, p
     if (grav != 0.) {
       R *rho = q, *pre = q + S::IPR * nc1;
       const double *rho0 = wp, *pre0 = wp + S::IPR * nc1;
-      for (int i = tid; i < nc1; i += nth) psv[i] = g.dx1f[i];
-      __syncthreads();
-      if (tid == 0) {
-        const double *dx = psv;
-        const double *rho = rho0, *pre = pre0;
-        double RdTv = pre[ie] / rho[ie];
-        double acc = pre[ie] * exp(grav * dx[ie] / (2 * RdTv));
-        psf[ie + 1] = acc;
-        for (int i = ie; i >= is; --i) {
-          acc = acc - grav * rho[i] * dx[i];
-          psf[i] = acc;
+      if (warp == 0) {
+        if (lane == 0) {
+          const double *dx = g.dx1f;
+          double RdTv = pre0[ie] / rho0[ie];
+          double acc = pre0[ie] * exp(grav * dx[ie] / (2 * RdTv));
+          psf[ie + 1] = acc;
+          // psf(i) = psf(i+1) - grav rho(i) dx(i), from the top, in the
+          // reference's order; operands fetched 8 levels ahead
+          int i = ie;
+          for (; i - 7 >= is; i -= 8) {
+            double x[8], d[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+              x[t] = grav * rho0[i - t];
+              d[t] = __ldg(dx + i - t);
+            }
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+              acc = acc - x[t] * d[t];
+              psf[i - t] = acc;
+            }
+          }
+          for (; i >= is; --i) {
+            acc = acc - grav * rho0[i] * dx[i];
+            psf[i] = acc;
+          }
+          const double gb = g.bc[0] == CANOE_BC_REFLECT ? -grav : grav;
+          for (int i = is - 1; i >= is - NG; --i) {
+            acc = acc - gb * rho0[i] * dx[i];
+            psf[i] = acc;
+          }
+          const double gt = g.bc[1] == CANOE_BC_REFLECT ? -grav : grav;
+          double p = psf[ie + 1];
+          for (int i = ie + 1; i <= ie + NG; ++i) {
+            p = p + gt * rho0[i] * dx[i];
+            psf[i + 1] = p;
+          }
         }
-        const double gb = g.bc[0] == CANOE_BC_REFLECT ? -grav : grav;
-        for (int i = is - 1; i >= is - NG; --i) {
-          acc = acc - gb * rho[i] * dx[i];
-          psf[i] = acc;
-        }
-        const double gt = g.bc[1] == CANOE_BC_REFLECT ? -grav : grav;
-        double p = psf[ie + 1];
-        for (int i = ie + 1; i <= ie + NG; ++i) {
-          p = p + gt * rho[i] * dx[i];
-          psf[i + 1] = p;
+      } else {
+        for (int t = tid - 32; t < (NV - 2) * ncell; t += nth - 32) {
+          recon(t / ncell + 1, is - 1 + t % ncell);  // slots 1 .. NV-2
         }
       }
       __syncthreads();
@@ -147,37 +230,32 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         double gm = th.rd * feps;
         psv[i] = pv;
         gam[i] = gm;
-        rho[i] = R(pre0[i] / (rho0[i] * gm));
-        pre[i] = R(pre0[i] - pv);
+        // outflow ghosts take the transformed values of the first / last
+        // interior cell (change_to_temperature.cpp:114-127)
+        const bool ob = (i < is && g.bc[0] == CANOE_BC_OUTFLOW);
+        const bool ot = (i > ie && g.bc[1] == CANOE_BC_OUTFLOW);
+        if (!ob && !ot) {
+          rho[i] = R(pre0[i] / (rho0[i] * gm));
+          pre[i] = R(pre0[i] - pv);
+        }
       }
       __syncthreads();
-      if (tid == 0) {
-        if (g.bc[0] == CANOE_BC_OUTFLOW)
-          for (int i = is - NG; i < is; ++i) {
-            rho[i] = rho[is];
-            pre[i] = pre[is];
+      if (g.bc[0] == CANOE_BC_OUTFLOW || g.bc[1] == CANOE_BC_OUTFLOW) {
+        for (int i = tid; i < nc1; i += nth) {
+          const bool ob = (i < is && g.bc[0] == CANOE_BC_OUTFLOW);
+          const bool ot = (i > ie && g.bc[1] == CANOE_BC_OUTFLOW);
+          if (ob || ot) {
+            const int c = ob ? is : ie;
+            rho[i] = rho[c];
+            pre[i] = pre[c];
           }
-        if (g.bc[1] == CANOE_BC_OUTFLOW)
-          for (int i = ie + 1; i <= ie + NG; ++i) {
-            rho[i] = rho[ie];
-            pre[i] = pre[ie];
-          }
+        }
+        __syncthreads();
       }
-    }
-    __syncthreads();
-    // P2
-    const int ncell = nx1 + 2;
-    for (int t = tid; t < NV * ncell; t += nth) {
-      const int n = t / ncell, c = is - 1 + t % ncell;
-      const R *qn = q + n * nc1;
-      R wl_, wr_;
-      if constexpr (RECON == CANOE_RECON_PPM)
-        ppm_cell(qn[c - 2], qn[c - 1], qn[c], qn[c + 1], qn[c + 2], wl_, wr_);
-      else
-        plm_cell_nu(qn[c - 1], qn[c], qn[c + 1], R(g.x1v[c - 1]), R(g.x1v[c]),
-                    R(g.x1v[c + 1]), R(g.x1f[c]), R(g.x1f[c + 1]), wl_, wr_);
-      WL[n * nc1 + c] = wl_;
-      WR[n * nc1 + c] = wr_;
+      for (int t = tid; t < 2 * ncell; t += nth)
+        recon(t < ncell ? 0 : S::IPR, is - 1 + t % ncell);
+    } else {
+      for (int t = tid; t < NV * ncell; t += nth) recon(t / ncell, is - 1 + t % ncell);
     }
     __syncthreads();
     // P3 (F aliases q, which nobody reads after P2)
@@ -226,7 +304,14 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         }
       }
     }
-    __syncthreads();
+    if (bulk && load_du) {
+      if (!__syncthreads_and(mbar_wait(mbar + 1, 0))) {
+        bail(1, 2);
+        return;
+      }
+    } else {
+      __syncthreads();
+    }
     // P4
     for (int i = is + tid; i <= ie; i += nth) {
       const int f0 = i - is;
@@ -248,22 +333,24 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         if constexpr (MODE == kColFluxOnly) {
           du[n * g.sv + base + i] = v;
         } else {
-          const double prev = g.f2 ? du[n * g.sv + base + i] : 0.;
-          dc[n * nx1 + f0] = prev + v;
+          const double prev = g.f2 ? dc[n * nc1 + i] : 0.;
+          dc[n * nc1 + i] = prev + v;
         }
       }
     }
     if constexpr (MODE == kColFluxOnly) return;
-  } else {
-    for (int n = 0; n < NV; ++n)
-      for (int r = tid; r < nx1; r += nth) dc[n * nx1 + r] = du[n * g.sv + base + is + r];
+  } else if (bulk) {
+    if (!__syncthreads_and(mbar_wait(mbar + 1, 0))) {
+      bail(1, 2);
+      return;
+    }
   }
   __syncthreads();
 
   if constexpr (N > 0) {
     constexpr int NN = ColRow<N>::NN, ROW = ColRow<N>::ROW;
     double *blk = un;                        // [nx1][ROW]
-    double *sA = blk + nx1 * ROW;            // [nx1+1][NN] |A| at faces is-1/2..ie+1/2
+    double *sA = sm + L.stg;                 // [nx1+1][NN] |A| at faces is-1/2..ie+1/2
     double *sJ = sA + (nx1 + 1) * NN;        // [nx1+2][NN] J of cells is-1..ie+1
     const double gm1 = th.gammad - 1.;
     const double dt = wght;
@@ -289,48 +376,6 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       }
     }
     __syncthreads();
-    // P5b: block rows (partial_correction.cpp:128-154); b of the first and c
-    // of the last row couple to ghosts: the reflecting condition folds them
-    // into a, and the sweep never uses them, so they are zeroed here
-    for (int r = tid; r < nx1; r += nth) {
-      const int i = is + r;
-      const double i2v = 1. / (2. * (g.dx1f[i] * g.dx2 * g.dx3));
-      double *row = blk + r * ROW;
-#pragma unroll
-      for (int e = 0; e < NN; ++e) {
-        const int rr = e / N, qq = e % N;
-        const double Am = sA[r * NN + e], Ap = sA[(r + 1) * NN + e];
-        const double Jm = sJ[r * NN + e], Jc = sJ[(r + 1) * NN + e], Jn = sJ[(r + 2) * NN + e];
-        double phi;
-        if (N == 3) phi = ((rr == 1 && qq == 0) || (rr == 2 && qq == 1)) ? grav : 0.;
-        else phi = ((rr == 1 && qq == 0) || (rr == 4 && qq == 1)) ? grav : 0.;
-        double a = (Am * area + Ap * area + (area - area) * Jc) * i2v + (rr == qq ? idt : 0.) - phi;
-        const double b = -(Am + Jm) * area * i2v;
-        const double c = -(Ap - Jn) * area * i2v;
-        if (i == is) a += (qq == 1 ? -b : b);
-        if (i == ie) a += (qq == 1 ? -c : c);
-        row[e] = a;
-        row[NN + e] = i == is ? 0. : b;
-        row[2 * NN + e] = i == ie ? 0. : c;
-      }
-      // right-hand side (forward_backward.hpp:24-41)
-      double r0 = dc[r];
-#pragma unroll
-      for (int n = 1; n <= NY; ++n) r0 += dc[n * nx1 + r];
-      double *rh = row + 3 * NN;
-      rh[0] = r0 / dt;
-      rh[1] = dc[S::IVX * nx1 + r] / dt;
-      if constexpr (N == 3) {
-        rh[2] = dc[S::IPR * nx1 + r] / dt;
-      } else {
-        rh[2] = dc[S::IVY * nx1 + r] / dt;
-        rh[3] = dc[S::IVZ * nx1 + r] / dt;
-        rh[4] = dc[S::IPR * nx1 + r] / dt;
-      }
-    }
-    __syncthreads();
-    // P6: block cyclic reduction.  Rows with (r+1) % 2s == 0 survive level s;
-    // rows with (r+1) % 2s == s are eliminated (their a is replaced by a^-1).
     auto ld = [&](const double *p) {
       M<N> m;
 #pragma unroll
@@ -351,84 +396,154 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
 #pragma unroll
       for (int e = 0; e < N; ++e) p[e] = v.a[e];
     };
-    // active rows are compacted onto the lowest threads so that a level
-    // with few rows occupies few warps
-    int s = 1;
-    for (; 2 * s - 1 < nx1; s *= 2) {
-      const int ne = (nx1 + s) / (2 * s);  // eliminated rows r = s-1 + 2 s m
-      for (int m = tid; m < ne; m += nth) {
-        const int r = s - 1 + 2 * s * m;
-        stm(blk + r * ROW, inv(ld(blk + r * ROW)));
-      }
-      __syncthreads();
-      const int nu = nx1 / (2 * s);  // surviving rows r = 2 s (m+1) - 1
-      for (int m = tid; m < nu; m += nth) {
-        const int r = 2 * s * (m + 1) - 1;
-        double *row = blk + r * ROW;
-        const double *lo = blk + (r - s) * ROW;
-        M<N> a = ld(row), b = ld(row + NN), c = ld(row + 2 * NN);
-        V<N> rh = ldv(row + 3 * NN);
-        // alpha = -b a_lo^-1
-        M<N> al = mm(b, ld(lo));
+    // P5b: block rows (partial_correction.cpp:128-154); b of the first and c
+    // of the last row couple to ghosts: the reflecting condition folds them
+    // into a, and the sweep never uses them, so they are zeroed here.  Rows
+    // that the first reduction level eliminates (r even) keep a^-1.
+    for (int r = tid; r < nx1; r += nth) {
+      const int i = is + r;
+      const double i2v = 1. / (2. * (g.dx1f[i] * g.dx2 * g.dx3));
+      double *row = blk + r * ROW;
+      M<N> am;
 #pragma unroll
-        for (int e = 0; e < NN; ++e) al.a[e / N][e % N] = -al.a[e / N][e % N];
-        M<N> t = mm(al, ld(lo + 2 * NN));
-        V<N> tv = mv(al, ldv(lo + 3 * NN));
+      for (int e = 0; e < NN; ++e) {
+        const int rr = e / N, qq = e % N;
+        const double Am = sA[r * NN + e], Ap = sA[(r + 1) * NN + e];
+        const double Jm = sJ[r * NN + e], Jc = sJ[(r + 1) * NN + e], Jn = sJ[(r + 2) * NN + e];
+        double phi;
+        if (N == 3) phi = ((rr == 1 && qq == 0) || (rr == 2 && qq == 1)) ? grav : 0.;
+        else phi = ((rr == 1 && qq == 0) || (rr == 4 && qq == 1)) ? grav : 0.;
+        double a = (Am * area + Ap * area + (area - area) * Jc) * i2v + (rr == qq ? idt : 0.) - phi;
+        const double b = -(Am + Jm) * area * i2v;
+        const double c = -(Ap - Jn) * area * i2v;
+        if (i == is) a += (qq == 1 ? -b : b);
+        if (i == ie) a += (qq == 1 ? -c : c);
+        am.a[rr][qq] = a;
+        row[NN + e] = i == is ? 0. : b;
+        row[2 * NN + e] = i == ie ? 0. : c;
+      }
+      stm(row, ((r & 1) == 0 && 1 < nx1) ? inv(am) : am);
+      // right-hand side (forward_backward.hpp:24-41)
+      double r0 = dc[i];
+#pragma unroll
+      for (int n = 1; n <= NY; ++n) r0 += dc[n * nc1 + i];
+      double *rh = row + 3 * NN;
+      rh[0] = r0 / dt;
+      rh[1] = dc[S::IVX * nc1 + i] / dt;
+      if constexpr (N == 3) {
+        rh[2] = dc[S::IPR * nc1 + i] / dt;
+      } else {
+        rh[2] = dc[S::IVY * nc1 + i] / dt;
+        rh[3] = dc[S::IVZ * nc1 + i] / dt;
+        rh[4] = dc[S::IPR * nc1 + i] / dt;
+      }
+    }
+    if (bulk) fence_proxy_async();
+    __syncthreads();
+    // u and u1 travel into the |A| / J area while the reduction runs
+    double *su = sA, *su1 = sA + NV * nc1;
+    const bool pre_u = bulk && MODE == kColStep;
+    if (pre_u && tid == 0) {
+      mbar_expect_tx(mbar + 2, (stage == 0 ? 1 : 2) * NV * row_bytes);
+      for (int n = 0; n < NV; ++n) bulk_g2s(su + n * nc1, u + n * g.sv + base, row_bytes, mbar + 2);
+      if (stage != 0)
+        for (int n = 0; n < NV; ++n)
+          bulk_g2s(su1 + n * nc1, u1 + n * g.sv + base, row_bytes, mbar + 2);
+    }
+    // P6: block cyclic reduction.  Level s updates the rows r = 2s(m+1) - 1
+    // from their neighbours r -/+ s, whose a was replaced by a^-1 when they
+    // were formed; a surviving row that the next level eliminates stores its
+    // new a^-1 right away.  Levels with at most 32 surviving rows run in
+    // warp 0 alone.
+    auto level = [&](int s, int m) {
+      const int r = 2 * s * (m + 1) - 1;
+      double *row = blk + r * ROW;
+      const double *lo = blk + (r - s) * ROW;
+      M<N> a = ld(row), b = ld(row + NN), c = ld(row + 2 * NN);
+      V<N> rh = ldv(row + 3 * NN);
+      // alpha = -b a_lo^-1
+      M<N> al = mm(b, ld(lo));
+#pragma unroll
+      for (int e = 0; e < NN; ++e) al.a[e / N][e % N] = -al.a[e / N][e % N];
+      M<N> t = mm(al, ld(lo + 2 * NN));
+      V<N> tv = mv(al, ldv(lo + 3 * NN));
+#pragma unroll
+      for (int e = 0; e < NN; ++e) a.a[e / N][e % N] += t.a[e / N][e % N];
+#pragma unroll
+      for (int e = 0; e < N; ++e) rh.a[e] += tv.a[e];
+      M<N> bn = mm(al, ld(lo + NN));
+      M<N> cn;
+      if (r + s < nx1) {
+        const double *hi = blk + (r + s) * ROW;
+        M<N> ga = mm(c, ld(hi));
+#pragma unroll
+        for (int e = 0; e < NN; ++e) ga.a[e / N][e % N] = -ga.a[e / N][e % N];
+        t = mm(ga, ld(hi + NN));
+        tv = mv(ga, ldv(hi + 3 * NN));
 #pragma unroll
         for (int e = 0; e < NN; ++e) a.a[e / N][e % N] += t.a[e / N][e % N];
 #pragma unroll
         for (int e = 0; e < N; ++e) rh.a[e] += tv.a[e];
-        M<N> bn = mm(al, ld(lo + NN));
-        M<N> cn;
-        if (r + s < nx1) {
-          const double *hi = blk + (r + s) * ROW;
-          M<N> ga = mm(c, ld(hi));
+        cn = mm(ga, ld(hi + 2 * NN));
+      } else {
 #pragma unroll
-          for (int e = 0; e < NN; ++e) ga.a[e / N][e % N] = -ga.a[e / N][e % N];
-          t = mm(ga, ld(hi + NN));
-          tv = mv(ga, ldv(hi + 3 * NN));
-#pragma unroll
-          for (int e = 0; e < NN; ++e) a.a[e / N][e % N] += t.a[e / N][e % N];
-#pragma unroll
-          for (int e = 0; e < N; ++e) rh.a[e] += tv.a[e];
-          cn = mm(ga, ld(hi + 2 * NN));
-        } else {
-#pragma unroll
-          for (int e = 0; e < NN; ++e) cn.a[e / N][e % N] = 0.;
-        }
-        stm(row, a);
-        stm(row + NN, bn);
-        stm(row + 2 * NN, cn);
-        stv(row + 3 * NN, rh);
+        for (int e = 0; e < NN; ++e) cn.a[e / N][e % N] = 0.;
       }
+      const bool next_elim = (m & 1) == 0 && 4 * s - 1 < nx1;
+      stm(row, next_elim ? inv(a) : a);
+      stm(row + NN, bn);
+      stm(row + 2 * NN, cn);
+      stv(row + 3 * NN, rh);
+    };
+    auto back = [&](int s, int m) {
+      const int r = s - 1 + 2 * s * m;
+      double *row = blk + r * ROW;
+      V<N> rh = ldv(row + 3 * NN);
+      if (r - s >= 0) {
+        V<N> t = mv(ld(row + NN), ldv(blk + (r - s) * ROW + 3 * NN));
+#pragma unroll
+        for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
+      }
+      if (r + s < nx1) {
+        V<N> t = mv(ld(row + 2 * NN), ldv(blk + (r + s) * ROW + 3 * NN));
+#pragma unroll
+        for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
+      }
+      stv(row + 3 * NN, mv(ld(row), rh));
+    };
+    int stop = 1;  // first s with 2 s - 1 >= nx1
+    while (2 * stop - 1 < nx1) stop *= 2;
+    int s = 1;
+    for (; s < stop && nx1 / (2 * s) > 32; s *= 2) {
+      for (int m = tid; m < nx1 / (2 * s); m += nth) level(s, m);
       __syncthreads();
     }
-    // the last surviving row r = s - 1 is decoupled
-    if (tid == 0) {
-      double *row = blk + (s - 1) * ROW;
-      M<N> ai = inv(ld(row));
-      stm(row, ai);
-      stv(row + 3 * NN, mv(ai, ldv(row + 3 * NN)));
+    const int s_warp = s;  // first level done by warp 0
+    // first back level done by all threads: the largest s with > 32 rows
+    int sb = 1;
+    while (2 * sb < stop && (nx1 + 2 * sb) / (4 * sb) > 32) sb *= 2;
+    if ((nx1 + sb) / (2 * sb) <= 32) sb = 0;  // every back level fits in warp 0
+    if (warp == 0) {
+      for (s = s_warp; s < stop; s *= 2) {
+        for (int m = lane; m < nx1 / (2 * s); m += 32) level(s, m);
+        __syncwarp();
+      }
+      // the last surviving row r = stop - 1 is decoupled
+      if (lane == 0) {
+        double *row = blk + (stop - 1) * ROW;
+        M<N> ai = inv(ld(row));
+        stm(row, ai);
+        stv(row + 3 * NN, mv(ai, ldv(row + 3 * NN)));
+      }
+      __syncwarp();
+      for (s = stop / 2; s >= 1 && s > sb; s /= 2) {
+        for (int m = lane; m < (nx1 + s) / (2 * s); m += 32) back(s, m);
+        __syncwarp();
+      }
     }
     __syncthreads();
-    for (s /= 2; s >= 1; s /= 2) {
-      const int ne = (nx1 + s) / (2 * s);
-      for (int m = tid; m < ne; m += nth) {
-        const int r = s - 1 + 2 * s * m;
-        double *row = blk + r * ROW;
-        V<N> rh = ldv(row + 3 * NN);
-        if (r - s >= 0) {
-          V<N> t = mv(ld(row + NN), ldv(blk + (r - s) * ROW + 3 * NN));
-#pragma unroll
-          for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
-        }
-        if (r + s < nx1) {
-          V<N> t = mv(ld(row + 2 * NN), ldv(blk + (r + s) * ROW + 3 * NN));
-#pragma unroll
-          for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
-        }
-        stv(row + 3 * NN, mv(ld(row), rh));
-      }
+    for (s = sb; s >= 1; s /= 2) {
+      for (int m = tid; m < (nx1 + s) / (2 * s); m += nth) back(s, m);
       __syncthreads();
     }
     // P7a: species correction (forward_backward.hpp:101-124) into dc
@@ -437,7 +552,7 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       const int i = is + r;
       double dv[NV];
 #pragma unroll
-      for (int n = 0; n < NV; ++n) dv[n] = dc[n * nx1 + r];
+      for (int n = 0; n < NV; ++n) dv[n] = dc[n * nc1 + i];
       double dens = dv[0];
 #pragma unroll
       for (int n = 1; n <= NY; ++n) dens += dv[n];
@@ -456,19 +571,45 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
 #pragma unroll
       for (int n = 1; n <= NY; ++n) dv[0] -= dv[n];
 #pragma unroll
-      for (int n = 0; n < NV; ++n) dc[n * nx1 + r] = dv[n];
+      for (int n = 0; n < NV; ++n) dc[n * nc1 + i] = dv[n];
     }
-    __syncthreads();
+    if (pre_u) {
+      if (!__syncthreads_and(mbar_wait(mbar + 2, 0))) {
+        bail(2, 3);
+        return;
+      }
+    } else {
+      __syncthreads();
+    }
+    if constexpr (MODE == kColStep) {
+      if (pre_u) {
+        for (int n = 0; n < NV; ++n)
+          for (int i = is + tid; i <= ie; i += nth) {
+            const int64_t x = n * g.sv + base + i;
+            const double uo = su[n * nc1 + i];
+            double ur;
+            if (stage == 0) {
+              u1[x] = uo;
+              ur = uo;
+            } else {
+              ur = su1[n * nc1 + i];
+            }
+            const double t = st.g1 * uo + st.g2 * ur;
+            u[x] = t + dc[n * nc1 + i];
+          }
+        return;
+      }
+    }
   }
 
   // P7b: write back
   if constexpr (MODE == kColSolveOnly) {
     for (int n = 0; n < NV; ++n)
-      for (int r = tid; r < nx1; r += nth) du[n * g.sv + base + is + r] = dc[n * nx1 + r];
+      for (int i = is + tid; i <= ie; i += nth) du[n * g.sv + base + i] = dc[n * nc1 + i];
   } else {
     for (int n = 0; n < NV; ++n)
-      for (int r = tid; r < nx1; r += nth) {
-        const int64_t x = n * g.sv + base + is + r;
+      for (int i = is + tid; i <= ie; i += nth) {
+        const int64_t x = n * g.sv + base + i;
         const double uo = u[x];
         double ur;
         if (stage == 0) {
@@ -478,7 +619,7 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
           ur = u1[x];
         }
         const double t = st.g1 * uo + st.g2 * ur;
-        u[x] = t + dc[n * nx1 + r];
+        u[x] = t + dc[n * nc1 + i];
       }
   }
 }
@@ -498,9 +639,14 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
     return CANOE_ERR_UNSUPPORTED;
   }
   const unsigned nblk = (unsigned)g.nx2 * (unsigned)g.nx3;
+  // bulk copies move whole pencil rows: 16-byte aligned bases and an even
+  // row length keep every row 16-byte aligned
+  auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };
+  Geom gg = g;
+  gg.bulk = (g.nc1 % 2 == 0) && al16(w) && al16(du) && al16(u) && al16(u1) ? 1 : 0;
   auto go = [&](auto kern) -> int {
     if (int rc = ensure_smem((const void *)kern, smem)) return rc;
-    kern<<<nblk, kColThreads, smem, st>>>(g, th, w, du, u, u1, dtp, s, stage, fout);
+    kern<<<nblk, kColThreads, smem, st>>>(gg, th, w, du, u, u1, dtp, s, stage, fout);
     CB_CUDA(cudaGetLastError());
     return 0;
   };

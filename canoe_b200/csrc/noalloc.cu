@@ -144,6 +144,7 @@ extern "C" int canoe_block_step_noalloc(const canoe_block_config_t *cfg, double 
   g.x1v = x1v;
   g.dx1f = dx1f;
   g.pref = pref;
+  g.err = err;
   int rc;
   // w (with ghosts) and the reference pressure profile of the state on entry
   if ((rc = launch_cons_to_prim(g, th, d_u, d_w, err, nullptr, cfg->cfl, cfg->implicit_flag,

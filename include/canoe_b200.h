@@ -48,7 +48,8 @@ enum canoe_errbit {
   CANOE_EBIT_NEG_PRESSURE = 2,
   CANOE_EBIT_NAN = 4,
   CANOE_EBIT_SATADJ_NOCONV = 8,
-  CANOE_EBIT_SATADJ_FALLBACK = 16
+  CANOE_EBIT_SATADJ_FALLBACK = 16,
+  CANOE_EBIT_TIMEOUT = 32        /* a bounded wait for an async copy gave up */
 };
 
 /* boundary flags (Athena BoundaryFlag subset used on this path) */
