@@ -46,23 +46,34 @@ __device__ __forceinline__ V<N> mv(const M<N> &x, const V<N> &y) {
   return r;
 }
 
+// entry (i, j) of the inverse of the row-major 3x3 matrix a (adjugate over
+// the determinant); inv(M<3>) and the entry-parallel reduction both use it
+__device__ __forceinline__ double inv3_entry(const double *a, int i, int j) {
+  const double c00 = a[4] * a[8] - a[5] * a[7];
+  const double c01 = a[5] * a[6] - a[3] * a[8];
+  const double c02 = a[3] * a[7] - a[4] * a[6];
+  const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+  const double id = 1. / det;
+  double num;
+  switch (3 * i + j) {
+    case 0: num = c00; break;
+    case 3: num = c01; break;
+    case 6: num = c02; break;
+    case 1: num = a[2] * a[7] - a[1] * a[8]; break;
+    case 4: num = a[0] * a[8] - a[2] * a[6]; break;
+    case 7: num = a[1] * a[6] - a[0] * a[7]; break;
+    case 2: num = a[1] * a[5] - a[2] * a[4]; break;
+    case 5: num = a[2] * a[3] - a[0] * a[5]; break;
+    default: num = a[0] * a[4] - a[1] * a[3]; break;
+  }
+  return num * id;
+}
+
 __device__ __forceinline__ M<3> inv(const M<3> &m) {
-  const double(*a)[3] = m.a;
-  double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
-  double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
-  double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
-  double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
-  double id = 1. / det;
+  const double *a = &m.a[0][0];
   M<3> r;
-  r.a[0][0] = c00 * id;
-  r.a[1][0] = c01 * id;
-  r.a[2][0] = c02 * id;
-  r.a[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id;
-  r.a[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id;
-  r.a[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id;
-  r.a[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id;
-  r.a[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id;
-  r.a[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) r.a[e / 3][e % 3] = inv3_entry(a, e / 3, e % 3);
   return r;
 }
 

@@ -158,6 +158,13 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         if (n == S::IPR) v -= pcst;
         q[n * nc1 + i] = R(v);
       }
+    // operands of the hydrostatic scan, staged where psv / gam go later:
+    // gam <- grav rho(i) (rounded as the scan's product), psv <- dx1f(i)
+    if (grav != 0.)
+      for (int i = tid; i < nc1; i += nth) {
+        gam[i] = grav * wp[i];
+        psv[i] = g.dx1f[i];
+      }
     __syncthreads();
     // P2 for variable n over the cells is-1 .. ie+1, items t0, t0+dt, ...
     const int ncell = nx1 + 2;
@@ -178,28 +185,45 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       const double *rho0 = wp, *pre0 = wp + S::IPR * nc1;
       if (warp == 0) {
         if (lane == 0) {
-          const double *dx = g.dx1f;
+          const double *dx = psv, *gr = gam;
           double RdTv = pre0[ie] / rho0[ie];
           double acc = pre0[ie] * exp(grav * dx[ie] / (2 * RdTv));
           psf[ie + 1] = acc;
           // psf(i) = psf(i+1) - grav rho(i) dx(i), from the top, in the
-          // reference's order; operands fetched 8 levels ahead
+          // reference's order.  Chunks of 8 levels: the operands of the next
+          // chunk are loaded before this chunk's results are stored.
           int i = ie;
-          for (; i - 7 >= is; i -= 8) {
+          if (i - 7 >= is) {
             double x[8], d[8];
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
-              x[t] = grav * rho0[i - t];
-              d[t] = __ldg(dx + i - t);
+              x[t] = gr[i - t];
+              d[t] = dx[i - t];
             }
+            for (;;) {
+              double pn[8];
 #pragma unroll
-            for (int t = 0; t < 8; ++t) {
-              acc = acc - x[t] * d[t];
-              psf[i - t] = acc;
+              for (int t = 0; t < 8; ++t) {
+                acc = acc - x[t] * d[t];
+                pn[t] = acc;
+              }
+              const int inext = i - 8;
+              const bool more = inext - 7 >= is;
+              if (more) {
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                  x[t] = gr[inext - t];
+                  d[t] = dx[inext - t];
+                }
+              }
+#pragma unroll
+              for (int t = 0; t < 8; ++t) psf[i - t] = pn[t];
+              i = inext;
+              if (!more) break;
             }
           }
           for (; i >= is; --i) {
-            acc = acc - grav * rho0[i] * dx[i];
+            acc = acc - gr[i] * dx[i];
             psf[i] = acc;
           }
           const double gb = g.bc[0] == CANOE_BC_REFLECT ? -grav : grav;
