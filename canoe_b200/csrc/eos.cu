@@ -400,6 +400,38 @@ __device__ __forceinline__ double mlp_features(const canoe_thermo_t &th, const d
   return ev / (th.rd / (th.gammad - 1.) * cvs);
 }
 
+// true when a condensable family of the cell is at or above saturation at
+// the all-vapour temperature tv (the lowest temperature the adjustment can
+// reach); otherwise the all-vapour state is the equilibrium, which the cold
+// start finds exactly, and a learned guess cannot help
+template <int NY>
+__device__ __forceinline__ bool may_condense(const canoe_thermo_t &th, const double *uc,
+                                             double tv) {
+  double rho = uc[0];
+#pragma unroll
+  for (int n = 1; n <= NY; ++n) rho += uc[n];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < (NY > 0 ? NY : 1); ++v) {
+    if (v >= th.nvapor) break;
+    const int ls = th.liq_slot[v], ss = th.ice_slot[v];
+    if (ls < 0 && ss < 0) continue;
+    double fam = 0.;
+#pragma unroll
+    for (int n = 1; n <= NY; ++n)
+      if (n == 1 + v || n == ls || n == ss) fam += uc[n];
+    const bool liquid = (ss < 0) || (ls >= 0 && tv >= th.t3[v]);
+    const double beta = liquid ? th.beta_l[v] : th.beta_s[v];
+    const double delta = liquid ? th.delta_l[v] : th.delta_s[v];
+    const double rv = th.rd * (1. + th.inv_mu_ratio_m1[v]);
+    const double ps =
+        th.p3[v] * exp(beta * (1. - th.t3[v] / tv) - delta * log(tv / th.t3[v]));
+    // vapour density of the family against saturation, with a 1e-3 margin
+    any = any || !(fam * rv * tv < (1. - 1e-3) * ps);
+  }
+  return any;
+}
+
 template <int NY, bool LEARNED>
 __global__ void __launch_bounds__(256)
     k_satadj(canoe_thermo_t th, canoe_satadj_opts_t o, double *__restrict__ u,
@@ -439,13 +471,22 @@ __global__ void __launch_bounds__(256)
   double tg = t_guess && active ? t_guess[t] : 0.;
   if constexpr (LEARNED) {
     // every lane of the warp takes part in the tensor-core inference
+    // (a warp whose cells all stay unsaturated skips the inference)
     float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f};
     double tdry = 0.;
-    if (active) tdry = mlp_features<NY>(th, uc, x);
+    bool need = false;
+    if (active) {
+      tdry = mlp_features<NY>(th, uc, x);
+      need = may_condense<NY>(th, uc, tdry);
+    }
+    tg = __longlong_as_double(0x7ff8000000000000LL);  // no guess: cold start
+    if (__any_sync(0xffffffffu, need)) {
 #pragma unroll
-    for (int q = 0; q < kMlpIn; ++q) x[q] = active ? (x[q] - mv.in_mean[q]) * mv.in_istd[q] : 0.f;
-    const float yn = mlp_warp_infer(x, sw1, sb1, sw2, sb2, sw3, mv.p[kMlpOffB3]);
-    tg = tdry + (double)(yn * mv.out_std + mv.out_mean);
+      for (int q = 0; q < kMlpIn; ++q)
+        x[q] = active ? (x[q] - mv.in_mean[q]) * mv.in_istd[q] : 0.f;
+      const float yn = mlp_warp_infer(x, sw1, sb1, sw2, sb2, sw3, mv.p[kMlpOffB3]);
+      if (need) tg = tdry + (double)(yn * mv.out_std + mv.out_mean);
+    }
     if (guess_out && active) guess_out[t] = tg;
   }
   if (active) {
