@@ -340,20 +340,18 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     for (int i = is + tid; i <= ie; i += nth) {
       const int f0 = i - is;
       const double idx = 1. / g.dx1f[i];
-      double fm0 = 0., fm1 = 0.;
-#pragma unroll
-      for (int n = 0; n <= NY; ++n) {
-        fm0 += (double)F[n * (nx1 + 1) + f0];
-        fm1 += (double)F[n * (nx1 + 1) + f0 + 1];
-      }
+      // constant x1 acceleration (HydroSourceTerms::ConstantAcceleration
+      // with canoe patches/25.constant_acc.patch:35-52): src = dt rho g on
+      // the x1 momentum, src v1 on the energy
+      const double gsrc = wght * wp[i] * grav;
 #pragma unroll
       for (int n = 0; n < NV; ++n) {
         double d = ((double)F[n * (nx1 + 1) + f0 + 1] - (double)F[n * (nx1 + 1) + f0]) * idx;
         // FP32 path: the momentum flux lacks psf, whose divergence is FP64
         if (PERT && n == S::IVX && grav != 0.) d += (psf[i + 1] - psf[i]) * idx;
         double v = -(wght * d);
-        if (n == S::IVX) v += wght * grav * wp[i];
-        if (n == S::IPR) v += wght * grav * 0.5 * (fm0 + fm1);
+        if (n == S::IVX) v += gsrc;
+        if (n == S::IPR) v += gsrc * wp[S::IVX * nc1 + i];
         if constexpr (MODE == kColFluxOnly) {
           du[n * g.sv + base + i] = v;
         } else {

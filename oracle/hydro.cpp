@@ -638,25 +638,21 @@ void add_flux_divergence(Block &b, double wght, std::vector<double> &du) {
         }
 }
 
-// Constant x1 gravity source (Athena HydroSourceTerms, external; restated):
-// momentum += dt g rho; energy += dt g (mass flux at the two x1 faces)/2,
-// with the mass flux summed over dry air and every species.
+// Constant x1 gravity source: HydroSourceTerms::ConstantAcceleration of
+// Athena++ (chengcli/athenapp @ 8c221aa, external) as patched by canoe
+// patches/25.constant_acc.patch:35-52: src = dt rho g with rho the total
+// density (prim(IDN); no passive scalars on this path), added to the x1
+// momentum, and src v1 added to the energy.
 void add_gravity_source(Block &b, double dt, std::vector<double> &du) {
   const double g = b.th.grav;
   if (g == 0.) return;
-  const int nc1 = b.nc1;
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = b.ks; k <= b.ke; ++k)
     for (int j = b.js; j <= b.je; ++j)
       for (int i = b.is; i <= b.ie; ++i) {
-        double fm0 = 0., fm1 = 0.;
-        for (int n = 0; n <= b.ny; ++n) {
-          size_t f1 = (((size_t)n * b.nc3 + k) * b.nc2 + j) * (nc1 + 1) + i;
-          fm0 += b.flx1[f1];
-          fm1 += b.flx1[f1 + 1];
-        }
-        du[b.idx(b.ivx, k, j, i)] += dt * g * b.w[b.idx(0, k, j, i)];
-        du[b.idx(b.ipr, k, j, i)] += dt * g * 0.5 * (fm0 + fm1);
+        double src = dt * b.w[b.idx(0, k, j, i)] * g;
+        du[b.idx(b.ivx, k, j, i)] += src;
+        du[b.idx(b.ipr, k, j, i)] += src * b.w[b.idx(b.ivx, k, j, i)];
       }
 }
 
