@@ -8,3 +8,4 @@ generators.
 from ._abi import CanoeError, load  # noqa: F401
 from . import thermo, problems  # noqa: F401
 from .block import MeshBlock  # noqa: F401
+from .shell import Shell  # noqa: F401

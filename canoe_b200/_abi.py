@@ -11,7 +11,7 @@ MAX_NY = 8
 MAX_VAPOR = 4
 NGHOST = 3
 
-BC_REFLECT, BC_PERIODIC, BC_OUTFLOW = 0, 1, 2
+BC_REFLECT, BC_PERIODIC, BC_OUTFLOW, BC_EXO3 = 0, 1, 2, 3
 RECON_PLM, RECON_PPM = 2, 3
 RS_LMARS, RS_HLLC = 0, 1
 FP64, FP32_PERTURBATION = 0, 1
@@ -44,6 +44,17 @@ class BlockConfig(ctypes.Structure):
         ("h_x1f", POINTER(c_double)),
         ("recon", c_int32), ("rsolver", c_int32), ("implicit_flag", c_int32),
         ("precision", c_int32), ("satadj", c_int32),
+        ("cfl", c_double),
+        ("thermo", Thermo),
+    ]
+
+
+class ShellConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx1", c_int32), ("nside", c_int32), ("bc_x1", c_int32 * 2),
+        ("h_x1f", POINTER(c_double)),
+        ("recon", c_int32), ("rsolver", c_int32), ("implicit_flag", c_int32),
+        ("precision", c_int32),
         ("cfl", c_double),
         ("thermo", Thermo),
     ]
@@ -95,6 +106,19 @@ SIGNATURES = [
     ("canoe_mlp_adam_step", c_int, [c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                     ctypes.c_float, c_void_p]),
     ("canoe_mlp_forward", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
+    ("canoe_shell_create", c_int, [POINTER(ShellConfig), POINTER(c_void_p)]),
+    ("canoe_shell_destroy", c_int, [c_void_p]),
+    ("canoe_shell_dims", c_int, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32),
+                                 POINTER(c_int32)]),
+    ("canoe_shell_set_stream", c_int, [c_void_p, c_void_p]),
+    ("canoe_shell_set_conserved", c_int, [c_void_p, c_void_p, c_int]),
+    ("canoe_shell_get_conserved", c_int, [c_void_p, c_void_p]),
+    ("canoe_shell_get_primitive", c_int, [c_void_p, c_void_p]),
+    ("canoe_shell_fill_ghosts", c_int, [c_void_p]),
+    ("canoe_shell_calculate_fluxes", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("canoe_shell_step", c_int, [c_void_p, c_double]),
+    ("canoe_shell_synchronize", c_int, [c_void_p]),
+    ("canoe_shell_error_word", c_int, [c_void_p, POINTER(c_uint32)]),
     ("canoe_saturation_adjust_learned", c_int, [POINTER(Thermo), POINTER(SatOpts), c_void_p,
                                                 c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
                                                 c_void_p, c_void_p]),

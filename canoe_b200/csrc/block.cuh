@@ -31,6 +31,20 @@ struct Geom {
   // set per launch: 1 when the pencil rows may be moved by bulk copies
   // (16-byte aligned arrays, nc1 even)
   int bulk;
+  // cubed-sphere panel: device geometry tables (kShellTabs arrays of
+  // nc3 * nc2 doubles, row-major [k][j]); null for a Cartesian block
+  const double *shell;
+};
+
+// geometry tables of a cubed-sphere panel (gnomonic_equiangle.cpp:140-222)
+enum ShellTab {
+  kTabCosC, kTabSinC,     // cell cosine / sine of the coordinate angle
+  kTabCosF2, kTabSinF2,   // at x2 faces
+  kTabCosF3, kTabSinF3,   // at x3 faces
+  kTabDx2A, kTabDx3A,     // angular widths of the cell
+  kTabDx2AF3, kTabDx3AF2, // angular widths along x3 / x2 faces
+  kTabCth1, kTabCth2, kTabCth3,  // flux-projection cosines (cell, x2 face, x3 face)
+  kShellTabs
 };
 
 // RK3 (SSPRK(3,3), Shu & Osher 1988) register weights per stage:

@@ -80,7 +80,14 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
 // copies issued at entry; u and u1 are fetched into the dead |A| / J area
 // while the cyclic reduction runs; the serial hydrostatic scan (one lane of
 // warp 0) overlaps the reconstruction of the variables it does not touch.
-template <int NY, int RECON, int RS, int N, int MODE, typename R>
+//
+// GEO = 1: a cubed-sphere panel (dry, FP64, HLLC): covariant kinetic energy
+// in the Riemann problem and the covariant flux projection
+// (hllc_transform.cpp:92-101, 245-272), radial face areas and cell volumes
+// (gnomonic_equiangle.cpp:224-432), the coordinate source terms
+// (AddCoordTermsDivergence, :833-878) and the implicit solve on velocities
+// projected to the local frame (solve_implicit_3d.cpp:105-137).
+template <int NY, int RECON, int RS, int N, int MODE, typename R, int GEO = 0>
 __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     k_x1col(Geom g, canoe_thermo_t th, const double *__restrict__ w,
             double *__restrict__ du, double *__restrict__ u, double *__restrict__ u1,
@@ -101,6 +108,9 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
   const int64_t base = (int64_t)k * g.sk + (int64_t)j * nc1;
   const int tid = threadIdx.x, nth = blockDim.x;
   const int warp = tid >> 5, lane = tid & 31;
+  // panel geometry of the column (GEO)
+  const int64_t nkj = (int64_t)g.nc3 * g.nc2;
+  auto tab = [&](int t, int kk, int jj) { return g.shell[t * nkj + (int64_t)kk * g.nc2 + jj]; };
   const double grav = th.grav;
   const double wght = st.beta * dtp[0];
   const bool bulk = g.bulk != 0;
@@ -313,10 +323,17 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
           wl[0] = pl / (wl[0] * gamma);
         }
       }
-      if constexpr (PERT)
+      if constexpr (GEO) {
+        hllc<R, NY, 0, true>(th, wl, wr, fx, R(tab(kTabCosC, k, j)));
+        const R cth = R(tab(kTabCth1, k, j));
+        const R ty = fx[S::IVY], tz = fx[S::IVZ];
+        fx[S::IVY] = ty + tz * cth;
+        fx[S::IVZ] = tz + ty * cth;
+      } else if constexpr (PERT) {
         riemann_pert<R, NY, RS, 0>(th, wl, wr, R(pf), fx);
-      else
+      } else {
         riemann<R, NY, RS, 0>(th, wl, wr, fx);
+      }
 #pragma unroll
       for (int n = 0; n < NV; ++n) F[n * (nx1 + 1) + (f - is)] = fx[n];
       if constexpr (MODE == kColFluxOnly) {
@@ -344,12 +361,45 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       // with canoe patches/25.constant_acc.patch:35-52): src = dt rho g on
       // the x1 momentum, src v1 on the energy
       const double gsrc = wght * wp[i] * grav;
+      // GEO: radial face areas, cell volume and coordinate sources
+      double a1m = 0., a1p = 0., vol = 1., csrc[3] = {0., 0., 0.};
+      if constexpr (GEO) {
+        const double d2 = tab(kTabDx2A, k, j), d3 = tab(kTabDx3A, k, j);
+        const double sc = tab(kTabSinC, k, j), cc = tab(kTabCosC, k, j);
+        const double xv = g.x1v[i], df = g.dx1f[i];
+        a1m = d2 * d3 * g.x1f[i] * g.x1f[i] * sc;
+        a1p = d2 * d3 * g.x1f[i + 1] * g.x1f[i + 1] * sc;
+        vol = df * d2 * d3 * xv * xv * sc;
+        const double a2m = xv * tab(kTabDx3AF2, k, j) * df;
+        const double a2p = xv * tab(kTabDx3AF2, k, j + 1) * df;
+        const double a3m = xv * tab(kTabDx2AF3, k, j) * df;
+        const double a3p = xv * tab(kTabDx2AF3, k + 1, j) * df;
+        const double v1 = wp[S::IVX * nc1 + i], v2 = wp[S::IVY * nc1 + i],
+                     v3 = wp[S::IVZ * nc1 + i];
+        const double pr = wp[S::IPR * nc1 + i], rho = wp[i];
+        const double v_2 = v2 + v3 * cc, v_3 = v3 + v2 * cc, sine2 = sc * sc;
+        const double x_ov_rD = (a2m * tab(kTabSinF2, k, j) - a2p * tab(kTabSinF2, k, j + 1)) / vol;
+        const double y_ov_rC = (a3m * tab(kTabSinF3, k, j) - a3p * tab(kTabSinF3, k + 1, j)) / vol;
+        csrc[0] = wght * ((2.0 * pr + rho * (v2 * v_2 + v3 * v_3)) / xv);
+        csrc[1] = wght * (-x_ov_rD * (pr + rho * v3 * v3 * sine2) - rho * v1 * v_2 / xv);
+        csrc[2] = wght * (-y_ov_rC * (pr + rho * v2 * v2 * sine2) - rho * v1 * v_3 / xv);
+      }
 #pragma unroll
       for (int n = 0; n < NV; ++n) {
-        double d = ((double)F[n * (nx1 + 1) + f0 + 1] - (double)F[n * (nx1 + 1) + f0]) * idx;
-        // FP32 path: the momentum flux lacks psf, whose divergence is FP64
-        if (PERT && n == S::IVX && grav != 0.) d += (psf[i + 1] - psf[i]) * idx;
-        double v = -(wght * d);
+        double v;
+        if constexpr (GEO) {
+          const double dfl = a1p * (double)F[n * (nx1 + 1) + f0 + 1] -
+                             a1m * (double)F[n * (nx1 + 1) + f0];
+          v = -(wght * dfl / vol);
+          if (n == S::IVX) v += csrc[0];
+          if (n == S::IVY) v += csrc[1];
+          if (n == S::IVZ) v += csrc[2];
+        } else {
+          double d = ((double)F[n * (nx1 + 1) + f0 + 1] - (double)F[n * (nx1 + 1) + f0]) * idx;
+          // FP32 path: the momentum flux lacks psf, whose divergence is FP64
+          if (PERT && n == S::IVX && grav != 0.) d += (psf[i + 1] - psf[i]) * idx;
+          v = -(wght * d);
+        }
         if (n == S::IVX) v += gsrc;
         if (n == S::IPR) v += gsrc * wp[S::IVX * nc1 + i];
         if constexpr (MODE == kColFluxOnly) {
@@ -378,12 +428,22 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     const double dt = wght;
     const double idt = 1. / dt;
     const double area = g.dx2 * g.dx3;
+    // GEO: the velocities of the solve are projected to the local frame
+    double pcos = 0., psin = 1.;
+    if constexpr (GEO) {
+      pcos = tab(kTabCosC, k, j);
+      psin = tab(kTabSinC, k, j);
+    }
     // P5a: |A| at face t (between cells is-1+t and is+t) and J of cell is-1+t
     for (int t = tid; t < nx1 + 2; t += nth) {
       const int ic = is - 1 + t;
       double wl[NV], wr[NV];
 #pragma unroll
       for (int n = 0; n < NV; ++n) wl[n] = wp[n * nc1 + ic];
+      if constexpr (GEO) {
+        wl[S::IVY] += wl[S::IVZ] * pcos;
+        wl[S::IVZ] *= psin;
+      }
       M<N> J;
       jacobian<N, NY>(J, gm1, wl);
 #pragma unroll
@@ -391,6 +451,10 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       if (t <= nx1) {
 #pragma unroll
         for (int n = 0; n < NV; ++n) wr[n] = wp[n * nc1 + ic + 1];
+        if constexpr (GEO) {
+          wr[S::IVY] += wr[S::IVZ] * pcos;
+          wr[S::IVZ] *= psin;
+        }
         M<N> A;
         abs_jacobian<N, NY>(A, th, gm1, wl, wr);
 #pragma unroll
@@ -424,7 +488,14 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     // that the first reduction level eliminates (r even) keep a^-1.
     for (int r = tid; r < nx1; r += nth) {
       const int i = is + r;
-      const double i2v = 1. / (2. * (g.dx1f[i] * g.dx2 * g.dx3));
+      double aL = area, aR = area;
+      double i2v = 1. / (2. * (g.dx1f[i] * g.dx2 * g.dx3));
+      if constexpr (GEO) {  // GetFace1Area / GetCellVolume
+        const double d2 = tab(kTabDx2A, k, j), d3 = tab(kTabDx3A, k, j), sc = tab(kTabSinC, k, j);
+        aL = d2 * d3 * g.x1f[i] * g.x1f[i] * sc;
+        aR = d2 * d3 * g.x1f[i + 1] * g.x1f[i + 1] * sc;
+        i2v = 1. / (2. * (g.dx1f[i] * d2 * d3 * g.x1v[i] * g.x1v[i] * sc));
+      }
       double *row = blk + r * ROW;
       M<N> am;
 #pragma unroll
@@ -435,9 +506,9 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         double phi;
         if (N == 3) phi = ((rr == 1 && qq == 0) || (rr == 2 && qq == 1)) ? grav : 0.;
         else phi = ((rr == 1 && qq == 0) || (rr == 4 && qq == 1)) ? grav : 0.;
-        double a = (Am * area + Ap * area + (area - area) * Jc) * i2v + (rr == qq ? idt : 0.) - phi;
-        const double b = -(Am + Jm) * area * i2v;
-        const double c = -(Ap - Jn) * area * i2v;
+        double a = (Am * aL + Ap * aR + (aR - aL) * Jc) * i2v + (rr == qq ? idt : 0.) - phi;
+        const double b = -(Am + Jm) * aL * i2v;
+        const double c = -(Ap - Jn) * aR * i2v;
         if (i == is) a += (qq == 1 ? -b : b);
         if (i == ie) a += (qq == 1 ? -c : c);
         am.a[rr][qq] = a;
@@ -673,6 +744,28 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
     return 0;
   };
   const bool ppm = recon == CANOE_RECON_PPM, hllc = rs == CANOE_RSOLVER_HLLC;
+  if (g.shell) {  // cubed-sphere panel: dry, FP64, HLLC
+    if constexpr (NY == 0 && sizeof(R) == 8) {
+      if (!hllc) {
+        set_error("the cubed-sphere panel uses the HLLC solver");
+        return CANOE_ERR_UNSUPPORTED;
+      }
+#define CB_GCOL(NIMPL, MODE) \
+  (ppm ? go(k_x1col<NY, 3, 1, NIMPL, MODE, R, 1>) : go(k_x1col<NY, 2, 1, NIMPL, MODE, R, 1>))
+      if (mode == kColFluxOnly) return CB_GCOL(0, kColFluxOnly);
+      if (mode == kColSolveOnly) {
+        set_error("solve-only mode is not provided on a cubed-sphere panel");
+        return CANOE_ERR_UNSUPPORTED;
+      }
+      if (nimpl == 0) return CB_GCOL(0, kColStep);
+      if (nimpl == 3) return CB_GCOL(3, kColStep);
+      return CB_GCOL(5, kColStep);
+#undef CB_GCOL
+    } else {
+      set_error("the cubed-sphere panel is dry and FP64");
+      return CANOE_ERR_UNSUPPORTED;
+    }
+  }
 #define CB_COL(NIMPL, MODE)                                                        \
   (ppm ? (hllc ? go(k_x1col<NY, 3, 1, NIMPL, MODE, R>) : go(k_x1col<NY, 3, 0, NIMPL, MODE, R>)) \
        : (hllc ? go(k_x1col<NY, 2, 1, NIMPL, MODE, R>) : go(k_x1col<NY, 2, 0, NIMPL, MODE, R>)))

@@ -156,10 +156,12 @@ __device__ __forceinline__ void lmars(const canoe_thermo_t &th, const R *wli,
 }
 
 // HLLC (Toro 2009, ch. 10): canoe src/snap/riemann/hllc_transform.cpp:
-// 25-233, Cartesian branch.
-template <typename R, int NY, int DIR>
+// 25-233.  COVKE: the x1 problem on a cubed-sphere panel, whose kinetic
+// energy is contravariant . covariant velocity with the cell's cosine
+// ke_cth (hllc_transform.cpp:92-101); the Cartesian branch otherwise.
+template <typename R, int NY, int DIR, bool COVKE = false>
 __device__ __forceinline__ void hllc(const canoe_thermo_t &th, const R *wl,
-                                     const R *wr, R *flx) {
+                                     const R *wr, R *flx, R ke_cth = R(0)) {
   using S = Slots<NY>;
   constexpr int IVX = S::IVX, IVY = S::IVY, IVZ = S::IVZ, IPR = S::IPR;
   constexpr int ivx = IVX + DIR;
@@ -189,8 +191,17 @@ __device__ __forceinline__ void hllc(const canoe_thermo_t &th, const R *wl,
   R kappar = R(1) / (gammar - R(1));
   R cl = sqrt(gammal * wli[IPR] / wli[0]);
   R cr = sqrt(gammar * wri[IPR] / wri[0]);
-  R KE_l = R(0.5) * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * wli[IVY] + wli[IVZ] * wli[IVZ]);
-  R KE_r = R(0.5) * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * wri[IVY] + wri[IVZ] * wri[IVZ]);
+  R KE_l, KE_r;
+  if constexpr (COVKE) {
+    R vy = wli[IVY] + wli[IVZ] * ke_cth, vz = wli[IVZ] + wli[IVY] * ke_cth;
+    KE_l = R(0.5) * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * vy + wli[IVZ] * vz);
+    vy = wri[IVY] + wri[IVZ] * ke_cth;
+    vz = wri[IVZ] + wri[IVY] * ke_cth;
+    KE_r = R(0.5) * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * vy + wri[IVZ] * vz);
+  } else {
+    KE_l = R(0.5) * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * wli[IVY] + wli[IVZ] * wli[IVZ]);
+    KE_r = R(0.5) * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * wri[IVY] + wri[IVZ] * wri[IVZ]);
+  }
   R el = wli[IPR] * kappal + KE_l;
   R er = wri[IPR] * kappar + KE_r;
   R rhoa = R(.5) * (wli[0] + wri[0]);

@@ -7,6 +7,10 @@ C2  3-D moist convection: dry adiabat capped by an isothermal layer, H2O at
     80 % relative humidity, liquid and ice at zero, seeded temperature noise
     near the ground (the moist-adiabat setup of src/snap/
     setup_moist_adiabatic_profile.cpp:7-90 restated for a dry adiabat).
+C3  cubed-sphere giant-planet shell: six panels, a dry H2-He adiabat through
+    165 K at 1 bar on levels uniform in log pressure from 100 bar to 0.1 bar,
+    seeded zonal jets of at most 5 m/s (panel velocities from the eastward
+    wind through CubedSphere::GetVyVz, cubed_sphere.cpp:138-151).
 C5  batched uneven blocks: C2's column physics on blocks of seeded sizes.
 
 Every generator returns a :class:`Problem`: the block configuration (a
@@ -20,7 +24,7 @@ import numpy as np
 
 from . import thermo as T
 from ._abi import (BC_PERIODIC, BC_REFLECT, FP64, NGHOST, RECON_PLM, RECON_PPM,
-                   RS_HLLC, RS_LMARS, BlockConfig)
+                   RS_HLLC, RS_LMARS, BlockConfig, ShellConfig)
 
 
 @dataclass
@@ -206,3 +210,97 @@ def moist3d(nx1=128, nx2=256, nx3=256, x1max=16.0e3, x2max=64.0e3, x3max=64.0e3,
     cfg, x1f = make_config(nx1, nx2, nx3, x1f, x2max / nx2, x3max / nx3, th, bc, recon,
                            rsolver, implicit_flag=implicit_flag, satadj=satadj, cfl=cfl)
     return Problem("C2-moist3d", cfg, x1f, u, w, dict(seed=seed))
+
+
+@dataclass
+class ShellProblem:
+    """A cubed-sphere shell: config, radial faces, conserved and primitive
+    state (6, NV, nc3, nc2, nc1) with covariant momenta in u and
+    contravariant velocities in w, ghost cells zero."""
+    name: str
+    cfg: ShellConfig
+    x1f: np.ndarray
+    u: np.ndarray
+    w: np.ndarray
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def nv(self):
+        return 5 + self.cfg.thermo.ny
+
+    def interior(self, a):
+        ng = NGHOST
+        n, nx1 = self.cfg.nside, self.cfg.nx1
+        return a[..., ng:ng + n, ng:ng + n, ng:ng + nx1]
+
+
+def shell_c3(nx1=64, nside=96, p_bot=100.0e5, p_top=0.1e5, t1bar=165.0, radius=7.1492e7,
+             jet=5.0, nmodes=8, seed=20240607, implicit_flag=1, recon=RECON_PPM, cfl=0.4,
+             th=None):
+    """C3: dry H2-He shell (g = 24.79 m/s^2, mu = 2.3 g/mol).  Radial faces
+    sit at pressures uniform in log p between p_bot and p_top on the dry
+    adiabat T = 165 K (p / 1 bar)^(R/cp), mapped to heights by the
+    hydrostatic relation dz = -cp dT / g of that adiabat; cell states follow
+    the same adiabat in height.  The eastward wind U(lat) sums nmodes seeded
+    cosine jets scaled to |U| <= jet; V = 0."""
+    from . import cubed_sphere as cs
+    th = th or T.giant_planet()
+    g = -th.grav
+    rd = th.rd
+    kappa = (th.gammad - 1.0) / th.gammad
+    cp = rd / kappa
+    pf = np.exp(np.linspace(np.log(p_bot), np.log(p_top), nx1 + 1))
+    tf = t1bar * (pf / 1.0e5) ** kappa
+    t_bot = tf[0]
+    zf = cp * (t_bot - tf) / g
+    x1f = radius + zf
+    x1v = 0.5 * (x1f[1:] + x1f[:-1])
+    tv = t_bot - g * (x1v - radius) / cp
+    pv = 1.0e5 * (tv / t1bar) ** (1.0 / kappa)
+    rhov = pv / (rd * tv)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    amp = rng.uniform(-1.0, 1.0, nmodes)
+    amp *= jet / np.abs(amp).sum()
+    n = nside + 2 * NGHOST
+    nc1 = nx1 + 2 * NGHOST
+    nv = 5
+    w = np.zeros((6, nv, n, n, nc1))
+    u = np.zeros_like(w)
+    _, av = cs.panel_angles(nside)
+    ing = slice(NGHOST, NGHOST + nside)
+    X = np.tan(av[ing])[None, :]     # x2 (j), last axis
+    Y = np.tan(av[ing])[:, None]     # x3 (k)
+    X, Y = np.broadcast_arrays(X, Y)
+    for p in range(6):
+        bid = p + 1
+        lat, lon = cs.latlon(bid, X, Y)
+        U = sum(a * np.cos((2 * m + 1) * lat) for m, a in enumerate(amp))
+        v2, v3 = cs.velocity_from_uv(bid, X, Y, U, np.zeros_like(U))
+        sl = (p, slice(None), ing, ing, slice(NGHOST, NGHOST + nx1))
+        wp = np.zeros((nv, nside, nside, nx1))
+        wp[0] = rhov[None, None, :]
+        wp[2] = v2[:, :, None]
+        wp[3] = v3[:, :, None]
+        wp[4] = pv[None, None, :]
+        w[sl] = wp
+        # PrimitiveToConserved with covariant momenta (patch 26)
+        cth = cs.cos_theta(X, Y)[:, :, None]
+        m1 = wp[1] * wp[0]
+        m2 = wp[2] * wp[0]
+        m3 = wp[3] * wp[0]
+        m2, m3 = m2 + m3 * cth, m3 + m2 * cth
+        up = np.zeros_like(wp)
+        up[0] = wp[0]
+        up[1], up[2], up[3] = m1, m2, m3
+        up[4] = wp[4] / (th.gammad - 1.0) + 0.5 * (m1 * wp[1] + m2 * wp[2] + m3 * wp[3])
+        u[sl] = up
+    cfg = ShellConfig()
+    cfg.nx1, cfg.nside = nx1, nside
+    cfg.bc_x1[0], cfg.bc_x1[1] = BC_REFLECT, BC_REFLECT
+    x1f = np.ascontiguousarray(x1f, dtype=np.float64)
+    cfg.h_x1f = x1f.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    cfg.recon, cfg.rsolver = recon, RS_HLLC
+    cfg.implicit_flag, cfg.precision = implicit_flag, FP64
+    cfg.cfl = cfl
+    cfg.thermo = th
+    return ShellProblem("C3-shell", cfg, x1f, u, w, dict(jet_amplitudes=amp, seed=seed))

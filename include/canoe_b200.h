@@ -53,7 +53,12 @@ enum canoe_errbit {
 };
 
 /* boundary flags (Athena BoundaryFlag subset used on this path) */
-enum canoe_bc { CANOE_BC_REFLECT = 0, CANOE_BC_PERIODIC = 1, CANOE_BC_OUTFLOW = 2 };
+enum canoe_bc {
+  CANOE_BC_REFLECT = 0,
+  CANOE_BC_PERIODIC = 1,
+  CANOE_BC_OUTFLOW = 2,
+  CANOE_BC_EXO3 = 3 /* cubed-sphere panel edge: ghosts filled by the exo3 exchange */
+};
 
 /* reconstruction order (Athena `xorder`): 2 = PLM, 3 = PPM */
 enum canoe_recon { CANOE_RECON_PLM = 2, CANOE_RECON_PPM = 3 };
@@ -116,6 +121,26 @@ typedef struct canoe_block_config {
 
 typedef struct canoe_block *canoe_block_t;
 typedef struct canoe_mlp *canoe_mlp_t;
+
+/* The six panels of an equiangular gnomonic cubed-sphere shell, one
+ * MeshBlock per panel (canoe src/exo3: CUBED_SPHERE build with NBLOCKS = 6,
+ * so cs_find_block_id.cpp:83-91 gives bound_lim = 0).  Panel p holds the
+ * reference's blockID p + 1; x2 and x3 are the panel's equiangular
+ * coordinates in [-pi/4, pi/4] with nside cells each, x1 the radius. */
+typedef struct canoe_shell_config {
+  int32_t nx1;          /* radial cells                                  */
+  int32_t nside;        /* cells along each panel edge (even)            */
+  int32_t bc_x1[2];     /* inner / outer radial boundary (canoe_bc)      */
+  const double *h_x1f;  /* nx1+1 radial faces [m] from the planet centre */
+  int32_t recon;        /* canoe_recon                                   */
+  int32_t rsolver;      /* CANOE_RSOLVER_HLLC (hllc_transform)           */
+  int32_t implicit_flag;/* bit0 X1, bit3 full 5x5                        */
+  int32_t precision;    /* canoe_precision                               */
+  double cfl;
+  canoe_thermo_t thermo;
+} canoe_shell_config_t;
+
+typedef struct canoe_shell *canoe_shell_t;
 
 /* ---------------- version / diagnostics ---------------- */
 const char *canoe_version(void);
@@ -298,6 +323,46 @@ int canoe_block_satadj_stats(canoe_block_t b, unsigned long long *h_stats);
 
 /* read and clear the block's device error word (canoe_errbit bits) */
 int canoe_block_error_word(canoe_block_t b, uint32_t *bits);
+
+/* ---------------- cubed-sphere shell (exo3) ----------------
+ * All six panels resident on one GPU in one array (6, NV, nc3, nc2, nc1),
+ * panel p = blockID - 1; conserved momenta covariant, primitive velocities
+ * contravariant (patches/26.adiabatic_hydro.patch).  The path is dry
+ * (ny = 0), HLLC and FP64, like the reference's exo3 build
+ * (cmake/examples/exo3.cmake: RSOLVER hllc_transform). */
+
+/* the six MeshBlocks of CubedSphere (src/exo3/cubed_sphere.cpp:25-33) with
+ * the GnomonicEquiangle tables (gnomonic_equiangle.cpp:24-222) */
+int canoe_shell_create(const canoe_shell_config_t *cfg, canoe_shell_t *out);
+int canoe_shell_destroy(canoe_shell_t s);
+int canoe_shell_dims(canoe_shell_t s, int32_t *nv, int32_t *nc1, int32_t *nc2,
+                     int32_t *nc3);
+int canoe_shell_set_stream(canoe_shell_t s, void *stream);
+
+/* load the host conserved state of all panels; fill != 0 then runs the panel
+ * ghost exchange and cons -> prim (the boundary step of the task list) */
+int canoe_shell_set_conserved(canoe_shell_t s, const double *h_u, int fill);
+int canoe_shell_get_conserved(canoe_shell_t s, double *h_u);
+int canoe_shell_get_primitive(canoe_shell_t s, double *h_w);
+
+/* Panel ghost exchange of the conserved state on device: what
+ * cs::PackData (src/exo3/cubed_sphere_utility.cpp:379-623, hooked at
+ * patches/33.bvals_cc_cpp.patch:21) with InteprolateX2/X3 (:100-376) and
+ * CubedSphere::TransformOX (cs_transform_ox.cpp:11-230) send over MPI, as one
+ * gather with interpolation and velocity rotation per ghost cell. */
+int canoe_shell_fill_ghosts(canoe_shell_t s);
+
+/* Hydro::CalculateFluxes of every panel with the CUBED_SPHERE branches of
+ * patches/19.calculate_fluxes.patch, including the L/R face-state swap of
+ * CubedSphere::SynchronizeFluxes{Send,Recv,Wait} (cubed_sphere.cpp:250-681).
+ * Device outputs (6, NV, nc3, nc2, nc1+1), (6, NV, nc3, nc2+1, nc1),
+ * (6, NV, nc3+1, nc2, nc1); d_f1 may be NULL. */
+int canoe_shell_calculate_fluxes(canoe_shell_t s, double *d_f1, double *d_f2, double *d_f3);
+
+/* One RK3 step of all panels with time step dt (> 0). */
+int canoe_shell_step(canoe_shell_t s, double dt);
+int canoe_shell_synchronize(canoe_shell_t s);
+int canoe_shell_error_word(canoe_shell_t s, uint32_t *bits);
 
 #ifdef __cplusplus
 }

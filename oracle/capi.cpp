@@ -184,4 +184,99 @@ double oracle_mlp_loss_grad(const double *params, int nh, const double *x,
   return loss;
 }
 
+// ---------------------------------------------------------------------------
+// cubed-sphere shell: state arrays are (6, nv, nc3, nc2, nc1)
+
+void *oracle_shell_new(const canoe_shell_config_t *cfg) {
+  try {
+    oracle::Shell *s = new oracle::Shell();
+    oracle::shell_init(*s, *cfg);
+    return s;
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+
+void oracle_shell_free(void *h) { delete static_cast<oracle::Shell *>(h); }
+
+static size_t panel_size(const oracle::Shell &s) { return s.p[0].u.size(); }
+
+int oracle_shell_set_conserved(void *h, const double *u) {
+  auto &s = *static_cast<oracle::Shell *>(h);
+  const size_t n = panel_size(s);
+  for (int p = 0; p < 6; ++p) std::memcpy(s.p[p].u.data(), u + p * n, n * sizeof(double));
+  return 0;
+}
+
+int oracle_shell_get(void *h, int which, double *out) {
+  auto &s = *static_cast<oracle::Shell *>(h);
+  const size_t n = panel_size(s);
+  for (int p = 0; p < 6; ++p)
+    std::memcpy(out + p * n, (which ? s.p[p].w : s.p[p].u).data(), n * sizeof(double));
+  return 0;
+}
+
+int oracle_shell_set_primitive(void *h, const double *w) {
+  auto &s = *static_cast<oracle::Shell *>(h);
+  const size_t n = panel_size(s);
+  for (int p = 0; p < 6; ++p) std::memcpy(s.p[p].w.data(), w + p * n, n * sizeof(double));
+  return 0;
+}
+
+int oracle_shell_fill_ghosts(void *h) {
+  try {
+    oracle::shell_fill_ghosts(*static_cast<oracle::Shell *>(h));
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  return 0;
+}
+
+int oracle_shell_cons_to_prim(void *h) {
+  oracle::shell_cons_to_prim(*static_cast<oracle::Shell *>(h));
+  return 0;
+}
+
+int oracle_shell_prim_to_cons(void *h) {
+  oracle::shell_prim_to_cons(*static_cast<oracle::Shell *>(h));
+  return 0;
+}
+
+// fluxes of the shell's current primitive state; f1/f2/f3 are
+// (6, nv, nc3, nc2, nc1+1), (6, nv, nc3, nc2+1, nc1), (6, nv, nc3+1, nc2, nc1)
+int oracle_shell_calculate_fluxes(void *h, double *f1, double *f2, double *f3) {
+  auto &s = *static_cast<oracle::Shell *>(h);
+  try {
+    for (int p = 0; p < 6; ++p) {
+      std::fill(s.p[p].flx1.begin(), s.p[p].flx1.end(), 0.);
+      std::fill(s.p[p].flx2.begin(), s.p[p].flx2.end(), 0.);
+      std::fill(s.p[p].flx3.begin(), s.p[p].flx3.end(), 0.);
+    }
+    oracle::shell_calculate_fluxes(s);
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  for (int p = 0; p < 6; ++p) {
+    const auto &b = s.p[p];
+    if (f1) std::memcpy(f1 + p * b.flx1.size(), b.flx1.data(), b.flx1.size() * sizeof(double));
+    if (f2) std::memcpy(f2 + p * b.flx2.size(), b.flx2.data(), b.flx2.size() * sizeof(double));
+    if (f3) std::memcpy(f3 + p * b.flx3.size(), b.flx3.data(), b.flx3.size() * sizeof(double));
+  }
+  return 0;
+}
+
+int oracle_shell_step(void *h, double dt, int nsteps) {
+  auto &s = *static_cast<oracle::Shell *>(h);
+  try {
+    for (int q = 0; q < nsteps; ++q) oracle::shell_step(s, dt);
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -199,7 +199,7 @@ void riemann_lmars(const canoe_thermo_t &th, int ivx, const double *wl,
 // HLLC: canoe src/snap/riemann/hllc_transform.cpp:25-233, Cartesian branch
 // (no GENERAL_EOS, no CUBED_SPHERE projection).
 void riemann_hllc(const canoe_thermo_t &th, int ivx, const double *wl,
-                  const double *wr, double *flx, int64_t n) {
+                  const double *wr, double *flx, int64_t n, const double *ke_cth) {
   int ny = th.ny, IVX = 1 + ny, IVY = 2 + ny, IVZ = 3 + ny, IPR = 4 + ny;
   int ivy = IVX + ((ivx - IVX) + 1) % 3;
   int ivz = IVX + ((ivx - IVX) + 2) % 3;
@@ -226,10 +226,22 @@ void riemann_hllc(const canoe_thermo_t &th, int ivx, const double *wl,
     double kappar = 1. / (gammar - 1.);
     double cl = sound_speed(th, wli);
     double cr = sound_speed(th, wri);
-    double KE_l = 0.5 * wli[0] *
-                  (wli[IVX] * wli[IVX] + wli[IVY] * wli[IVY] + wli[IVZ] * wli[IVZ]);
-    double KE_r = 0.5 * wri[0] *
-                  (wri[IVX] * wri[IVX] + wri[IVY] * wri[IVY] + wri[IVZ] * wri[IVZ]);
+    double KE_l, KE_r;
+    if (ke_cth) {
+      // x1 on a cubed-sphere panel: contravariant . covariant velocity
+      // (ContravariantVectorToCovariant, cubed_sphere.cpp:225-238)
+      const double cth = *ke_cth;
+      double vy = wli[IVY] + wli[IVZ] * cth, vz = wli[IVZ] + wli[IVY] * cth;
+      KE_l = 0.5 * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * vy + wli[IVZ] * vz);
+      vy = wri[IVY] + wri[IVZ] * cth;
+      vz = wri[IVZ] + wri[IVY] * cth;
+      KE_r = 0.5 * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * vy + wri[IVZ] * vz);
+    } else {
+      KE_l = 0.5 * wli[0] *
+             (wli[IVX] * wli[IVX] + wli[IVY] * wli[IVY] + wli[IVZ] * wli[IVZ]);
+      KE_r = 0.5 * wri[0] *
+             (wri[IVX] * wri[IVX] + wri[IVY] * wri[IVY] + wri[IVZ] * wri[IVZ]);
+    }
     double el = wli[IPR] * kappal + KE_l;
     double er = wri[IPR] * kappar + KE_r;
     double rhoa = .5 * (wli[0] + wri[0]);
@@ -322,7 +334,7 @@ static void plm_line_nonuniform(const double *q, const double *xv,
 }
 
 // PLM, uniform spacing (x2, x3).
-static void plm_line(const double *q, int lo, int hi, double *ql, double *qr) {
+void plm_line(const double *q, int lo, int hi, double *ql, double *qr) {
   for (int c = lo - 1; c <= hi; ++c) {
     double dwl = q[c] - q[c - 1];
     double dwr = q[c + 1] - q[c];
@@ -344,7 +356,7 @@ static inline double ppm_slope(double qm, double q0, double qp) {
   return std::copysign(lim, dwc);
 }
 
-static void ppm_line(const double *q, int lo, int hi, double *ql, double *qr) {
+void ppm_line(const double *q, int lo, int hi, double *ql, double *qr) {
   for (int c = lo - 1; c <= hi; ++c) {
     double dm_m = ppm_slope(q[c - 2], q[c - 1], q[c]);
     double dm_0 = ppm_slope(q[c - 1], q[c], q[c + 1]);
@@ -535,16 +547,32 @@ static void flux_x1_pencil(Block &b, int k, int j, std::vector<double> &q,
       pr[n * nf + f] = wr[n * (nc1 + 1) + lo + f];
     }
   fx.resize(nv * nf);
-  riemann(b, b.ivx, pl.data(), pr.data(), fx.data(), nf);
+  if (b.geo) {
+    // cubed-sphere panel: covariant kinetic energy in the x1 Riemann problem
+    // (hllc_transform.cpp:92-101) and the contravariant -> covariant
+    // projection of the transverse momentum fluxes (:245-272)
+    const double x = std::tan(b.geo->x2v[j]), y = std::tan(b.geo->x3v[k]);
+    const double Ck = std::sqrt(x * x + 1), Dk = std::sqrt(y * y + 1);
+    const double cth_ke = -x * y / (Ck * Dk);
+    riemann_hllc(b.th, b.ivx, pl.data(), pr.data(), fx.data(), nf, &cth_ke);
+    const double C = std::sqrt(1. + x * x), D = std::sqrt(1. + y * y);
+    const double cth = -x * y / C / D;
+    for (int f = 0; f < nf; ++f) {
+      const double ty = fx[b.ivy * nf + f], tz = fx[b.ivz * nf + f];
+      fx[b.ivy * nf + f] = ty + tz * cth;
+      fx[b.ivz * nf + f] = tz + ty * cth;
+    }
+  } else {
+    riemann(b, b.ivx, pl.data(), pr.data(), fx.data(), nf);
+  }
   for (int n = 0; n < nv; ++n)
     for (int f = 0; f < nf; ++f)
       b.flx1[(((size_t)n * b.nc3 + k) * b.nc2 + j) * (nc1 + 1) + lo + f] =
           fx[n * nf + f];
 }
 
-void calculate_fluxes(Block &b) {
+void calculate_fluxes_x1_only(Block &b) {
   const int nv = b.nv;
-  // x1
 #pragma omp parallel
   {
     std::vector<double> q(nv * b.nc1), wl(nv * (b.nc1 + 1)), wr(nv * (b.nc1 + 1)), fx;
@@ -552,6 +580,11 @@ void calculate_fluxes(Block &b) {
     for (int k = b.ks; k <= b.ke; ++k)
       for (int j = b.js; j <= b.je; ++j) flux_x1_pencil(b, k, j, q, wl, wr, fx);
   }
+}
+
+void calculate_fluxes(Block &b) {
+  const int nv = b.nv;
+  calculate_fluxes_x1_only(b);
   // x2: lines along j for every interior (k, i)
   if (b.f2) {
 #pragma omp parallel

@@ -185,8 +185,19 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
   const int nc1 = b.nc1, nv = b.nv, ny = b.ny, IVX = b.ivx, IPR = b.ipr;
   const int is = b.is, ie = b.ie;
   const size_t s = b.cells();
+  // a cubed-sphere panel projects the velocities onto the local frame
+  // for the solve (solve_implicit_3d.cpp:105-117)
+  double cos_t = 0., sin_t = 1.;
+  if (b.geo) {
+    cos_t = b.geo->cosc[b.geo->kj(k, j)];
+    sin_t = b.geo->sinc[b.geo->kj(k, j)];
+  }
   auto W = [&](int i, double *out) {
     for (int n = 0; n < nv; ++n) out[n] = b.w[b.idx(0, k, j, i) + n * s];
+    if (b.geo) {
+      out[IVX + 1] += out[IVX + 2] * cos_t;
+      out[IVX + 2] *= sin_t;
+    }
   };
   const double gm1 = b.th.gammad - 1.;
   const double grav = b.th.grav;
@@ -232,6 +243,11 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
     abs_jacobian(full, prim, cs, gm1, ny);
     Ap = reduce<N>(full);
     double aleft = area, aright = area, vol = b.dx1f[i] * b.dx2 * b.dx3;
+    if (b.geo) {  // GetFace1Area / GetCellVolume of the panel
+      aleft = shell_face1_area(b, k, j, i);
+      aright = shell_face1_area(b, k, j, i + 1);
+      vol = shell_cell_volume(b, k, j, i);
+    }
     for (int r = 0; r < N; ++r)
       for (int q = 0; q < N; ++q) {
         a[i].a[r][q] = (Am.a[r][q] * aleft + Ap.a[r][q] * aright +

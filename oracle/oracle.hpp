@@ -28,6 +28,18 @@ namespace oracle {
 
 constexpr int NG = CANOE_NGHOST;
 
+// Panel geometry of an equiangular gnomonic cubed sphere
+// (canoe src/exo3/gnomonic_equiangle.cpp:24-222); the six panels of a shell
+// share one.  Angles x2, x3 in [-pi/4, pi/4]; (k, j) tables are row-major
+// [k * nc2 + j].
+struct ShellGeo {
+  int N = 0, nc2 = 0, nc3 = 0;
+  std::vector<double> x2f, x2v, x3f, x3v;
+  std::vector<double> cosc, sinc, cosf2, sinf2, cosf3, sinf3;
+  std::vector<double> dx2a, dx3a, dx2a_f3, dx3a_f2;
+  size_t kj(int k, int j) const { return (size_t)k * nc2 + j; }
+};
+
 struct Block {
   canoe_block_config_t cfg;
   canoe_thermo_t th;
@@ -45,6 +57,9 @@ struct Block {
   // decomposition scratch (canoe decomposition.hpp:77-87)
   std::vector<double> psf, psv, gam;  // (nc3,nc2,nc1+1), (nc3,nc2,nc1) x2
   bool fix_roundtrip = true;  // write the T/p' round trip back into w
+  // cubed-sphere panel: geometry and blockID - 1 (nullptr / -1 otherwise)
+  const ShellGeo *geo = nullptr;
+  int panel = -1;
 
   size_t cells() const { return (size_t)nc3 * nc2 * nc1; }
   size_t idx(int n, int k, int j, int i) const {
@@ -67,18 +82,50 @@ double temperature_of_prim(const canoe_thermo_t &th, const double *w,
 // Riemann solvers on (nv, n) face arrays ------------------------------------
 void riemann_lmars(const canoe_thermo_t &th, int ivx, const double *wl,
                    const double *wr, double *flx, int64_t n);
+// ke_cth: cosine of the cell for the covariant kinetic energy of the x1
+// Riemann problem on a cubed-sphere panel (hllc_transform.cpp:92-101); null
+// elsewhere
 void riemann_hllc(const canoe_thermo_t &th, int ivx, const double *wl,
-                  const double *wr, double *flx, int64_t n);
+                  const double *wr, double *flx, int64_t n,
+                  const double *ke_cth = nullptr);
+
+// reconstruction along one line: cell values q, faces f between cells f-1
+// and f; ql[f] / qr[f] left / right of face f for faces lo..hi
+void plm_line(const double *q, int lo, int hi, double *ql, double *qr);
+void ppm_line(const double *q, int lo, int hi, double *ql, double *qr);
 
 // block-level -----------------------------------------------------------------
 void apply_bc(Block &b, std::vector<double> &w);
 void cons_to_prim_block(Block &b);
 void calculate_fluxes(Block &b);
+void calculate_fluxes_x1_only(Block &b);
 void add_flux_divergence(Block &b, double wght, std::vector<double> &du);
 void add_gravity_source(Block &b, double dt, std::vector<double> &du);
 void solve_implicit(Block &b, std::vector<double> &du, double dt);
 double new_dt(const Block &b);
 void step(Block &b, double dt);
+
+// cubed-sphere shell (exo3.cpp) ------------------------------------------------
+struct Shell {
+  canoe_shell_config_t cfg;
+  int N = 0, nv = 0;
+  ShellGeo geo;
+  Block p[6];
+  // x2 / x3 face states of every panel (CubedSphere L3DValues / R3DValues,
+  // cubed_sphere.hpp:67): (nv, nc3, nc2 + 1, nc1) and (nv, nc3 + 1, nc2, nc1)
+  std::vector<double> L2[6], R2[6], L3[6], R3[6];
+};
+void shell_init(Shell &s, const canoe_shell_config_t &cfg);
+void shell_fill_ghosts(Shell &s);
+void shell_cons_to_prim(Shell &s);
+void shell_prim_to_cons(Shell &s);
+void shell_calculate_fluxes(Shell &s);
+void shell_step(Shell &s, double dt);
+void shell_swap_lr(Shell &s);
+void shell_add_divergence(Block &b, double wght, std::vector<double> &du);
+// radial geometry of a panel cell (gnomonic_equiangle.cpp:224-432)
+double shell_face1_area(const Block &b, int k, int j, int i);
+double shell_cell_volume(const Block &b, int k, int j, int i);
 
 // saturation adjustment (one cell, conserved, stride between variables) ----
 struct SatResult {

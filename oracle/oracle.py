@@ -10,7 +10,7 @@ from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_void_
 
 import numpy as np
 
-from canoe_b200._abi import BlockConfig, SatOpts, Thermo
+from canoe_b200._abi import BlockConfig, SatOpts, ShellConfig, Thermo
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "liboracle.so")
@@ -51,6 +51,16 @@ def load():
                                   c_void_p, c_void_p, c_void_p]),
         ("oracle_mlp_forward", c_int, [c_void_p, c_int, c_void_p, c_int64, c_void_p]),
         ("oracle_mlp_loss_grad", c_double, [c_void_p, c_int, c_void_p, c_void_p, c_int64, c_void_p]),
+        ("oracle_shell_new", c_void_p, [POINTER(ShellConfig)]),
+        ("oracle_shell_free", None, [c_void_p]),
+        ("oracle_shell_set_conserved", c_int, [c_void_p, c_void_p]),
+        ("oracle_shell_set_primitive", c_int, [c_void_p, c_void_p]),
+        ("oracle_shell_get", c_int, [c_void_p, c_int, c_void_p]),
+        ("oracle_shell_fill_ghosts", c_int, [c_void_p]),
+        ("oracle_shell_cons_to_prim", c_int, [c_void_p]),
+        ("oracle_shell_prim_to_cons", c_int, [c_void_p]),
+        ("oracle_shell_calculate_fluxes", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        ("oracle_shell_step", c_int, [c_void_p, c_double, c_int]),
     ]
     for name, res, args in sig:
         fn = getattr(lib, name)
@@ -186,3 +196,61 @@ def mlp_loss_grad(params, nh, x, y):
     loss = load().oracle_mlp_loss_grad(p.ctypes.data, nh, x.ctypes.data, y.ctypes.data,
                                        x.shape[0], g.ctypes.data)
     return loss, g
+
+
+class OracleShell:
+    """The oracle's six-panel cubed-sphere shell (FP64)."""
+
+    def __init__(self, problem):
+        self.lib = load()
+        self.problem = problem
+        self.h = self.lib.oracle_shell_new(ctypes.byref(problem.cfg))
+        if not self.h:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        self.shape = problem.u.shape
+        self.set_conserved(problem.u)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_shell_free(self.h)
+            self.h = None
+
+    def _check(self, rc):
+        assert rc == 0, self.lib.oracle_last_error().decode()
+
+    def set_conserved(self, u, fill=True):
+        """load u; by default fill the panel ghosts and compute w"""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.shape == self.shape
+        self.lib.oracle_shell_set_conserved(self.h, u.ctypes.data)
+        if fill:
+            self.fill_ghosts()
+            self.cons_to_prim()
+
+    def fill_ghosts(self):
+        self._check(self.lib.oracle_shell_fill_ghosts(self.h))
+
+    def cons_to_prim(self):
+        self._check(self.lib.oracle_shell_cons_to_prim(self.h))
+
+    def conserved(self):
+        out = np.empty(self.shape)
+        self.lib.oracle_shell_get(self.h, 0, out.ctypes.data)
+        return out
+
+    def primitive(self):
+        out = np.empty(self.shape)
+        self.lib.oracle_shell_get(self.h, 1, out.ctypes.data)
+        return out
+
+    def calculate_fluxes(self):
+        six, nv, n3, n2, n1 = self.shape
+        f1 = np.zeros((6, nv, n3, n2, n1 + 1))
+        f2 = np.zeros((6, nv, n3, n2 + 1, n1))
+        f3 = np.zeros((6, nv, n3 + 1, n2, n1))
+        self._check(self.lib.oracle_shell_calculate_fluxes(self.h, f1.ctypes.data,
+                                                           f2.ctypes.data, f3.ctypes.data))
+        return f1, f2, f3
+
+    def step(self, dt, nsteps=1):
+        self._check(self.lib.oracle_shell_step(self.h, float(dt), int(nsteps)))
