@@ -212,6 +212,56 @@ def c4_report(net, th, ncells=1 << 24):
     return out
 
 
+def c3_report(steps=10, warmup=3, nx1=64, nside=96, dt=60.0):
+    """C3: the six-panel cubed-sphere shell (FP64, PPM + HLLC, implicit x1)
+    stepped on device with the panel exchange; zone-cycles/s and the ghost
+    exchange's bandwidth (algorithmic bytes: two source reads and one write
+    of NV doubles per ghost cell)."""
+    import torch
+    from canoe_b200 import Shell, problems
+    from canoe_b200._abi import check
+    p = problems.shell_c3(nx1=nx1, nside=nside)
+    sh = Shell(p)
+    stream = torch.cuda.Stream()
+    check(sh.lib.canoe_shell_set_stream(sh.h, ctypes.c_void_p(stream.cuda_stream)))
+    cells = 6 * nside * nside * nx1
+    out = {"cells": cells, "config": f"6 x {nside}x{nside} x {nx1}, PPM + HLLC, implicit x1 "
+           "partial 3x3, FP64 (the shell has no FP32 path)", "dt": dt}
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            sh.step(dt)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            sh.step(dt)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out["ms_per_step"] = ms / steps
+        out["value"] = cells * steps / (ms * 1e-3)
+        out["unit"] = UNIT
+        # the ghost exchange alone, repeated (its inputs are the panels'
+        # edge layers, 53 MB per call at full size: they stay in L2)
+        reps = 50
+        e0.record(stream)
+        for _ in range(reps):
+            check(sh.lib.canoe_shell_fill_ghosts(sh.h))
+        e1.record(stream)
+        e1.synchronize()
+        us = e0.elapsed_time(e1) * 1e3 / reps
+        ghosts = 6 * 4 * 3 * nside * nx1
+        byts = 3 * 8 * 5 * ghosts
+        out["ghost_exchange"] = {"us_per_call": us, "ghost_cells": ghosts,
+                                 "algorithmic_bytes": byts, "gbs": byts / (us * 1e-6) / 1e9,
+                                 "note": "repeated calls: source layers L2-resident"}
+    w = p.interior(sh.primitive())
+    out["finite"] = bool(np.isfinite(w).all())
+    out["error_word"] = sh.error_word()
+    sh.close()
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -252,6 +302,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-c4", action="store_true")
+    ap.add_argument("--no-c3", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -418,6 +469,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args)
     c4 = None
+    c3 = None
+    if rank == 0 and not args.no_c3:
+        c3 = c3_report()
     if rank == 0 and not args.no_c4:
         c4 = c4_report(net, p.cfg.thermo)
     if dist:
@@ -435,6 +489,7 @@ def main():
                 (value / other["value"]) if args.precision == "mixed" else other["value"] / value,
             "l2_error_mixed_vs_fp64": l2, "saturation_adjustment": sat,
             "c4_learned_warm_start": c4,
+            "c3_cubed_sphere_shell": c3,
             "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
             "error_word": err}
     print(json.dumps(line), flush=True)
