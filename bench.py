@@ -262,6 +262,69 @@ def c3_report(steps=10, warmup=3, nx1=64, nside=96, dt=60.0):
     return out
 
 
+def c5_report(net, steps=5, warmup=2):
+    """C5: 48 uneven blocks of C2 physics stepped as one CUDA graph with
+    autotuned threads per x1 pencil, mixed + learned and plain FP64, against
+    the same blocks stepped one after another with default launches."""
+    import torch
+    from canoe_b200 import Batch, MeshBlock, problems
+    ps = problems.batch_c5()
+    cells = sum(p.cfg.nx1 * p.cfg.nx2 * p.cfg.nx3 for p in ps)
+    out = {"blocks": len(ps), "cells": cells,
+           "sizes": "nz logU[32,256], nh logU[16,128] square, seed 20240605"}
+
+    def make(precision):
+        blocks = []
+        for p in ps:
+            p.cfg.precision = 1 if precision == "mixed" else 0
+            b = MeshBlock(p)
+            if precision == "mixed":
+                b.set_mlp(net)
+            b.set_fixed_dt(b.new_dt())
+            blocks.append(b)
+        return blocks
+
+    def timed(fn, sync):
+        for _ in range(warmup):
+            fn()
+        sync()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        sync()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    for prec in ("mixed", "fp64"):
+        blocks = make(prec)
+        bt = Batch(blocks, graph=False)
+        # one block after another on one stream, default launches
+        def seq():
+            for b in blocks:
+                b.step()
+                b.synchronize()
+        ms_seq = timed(seq, lambda: None)
+        choice = bt.autotune()
+        bt.use_graph(True)
+        ms_graph = timed(bt.step, bt.synchronize)
+        errs = [b.error_word() for b in blocks]
+        out[prec] = {"ms_per_step": ms_graph, "value": cells / (ms_graph * 1e-3),
+                     "sequential_ms_per_step": ms_seq,
+                     "sequential_value": cells / (ms_seq * 1e-3),
+                     "threads_per_pencil": {str(t): int((choice == t).sum())
+                                            for t in (64, 96, 128, 160)},
+                     "error_words": int(np.bitwise_or.reduce(np.array(errs)))}
+        bt.close()
+        for b in blocks:
+            b.close()
+    out["unit"] = UNIT
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -303,6 +366,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-c4", action="store_true")
     ap.add_argument("--no-c3", action="store_true")
+    ap.add_argument("--no-c5", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -472,6 +536,9 @@ def main():
     c3 = None
     if rank == 0 and not args.no_c3:
         c3 = c3_report()
+    c5 = None
+    if rank == 0 and not args.no_c5:
+        c5 = c5_report(net)
     if rank == 0 and not args.no_c4:
         c4 = c4_report(net, p.cfg.thermo)
     if dist:
@@ -490,6 +557,7 @@ def main():
             "l2_error_mixed_vs_fp64": l2, "saturation_adjustment": sat,
             "c4_learned_warm_start": c4,
             "c3_cubed_sphere_shell": c3,
+            "c5_batched_blocks": c5,
             "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
             "error_word": err}
     print(json.dumps(line), flush=True)

@@ -9,3 +9,4 @@ from ._abi import CanoeError, load  # noqa: F401
 from . import thermo, problems  # noqa: F401
 from .block import MeshBlock  # noqa: F401
 from .shell import Shell  # noqa: F401
+from .batch import Batch  # noqa: F401

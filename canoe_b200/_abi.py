@@ -106,6 +106,13 @@ SIGNATURES = [
     ("canoe_mlp_adam_step", c_int, [c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                     ctypes.c_float, c_void_p]),
     ("canoe_mlp_forward", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
+    ("canoe_block_set_column_threads", c_int, [c_void_p, c_int]),
+    ("canoe_batch_create", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    ("canoe_batch_destroy", c_int, [c_void_p]),
+    ("canoe_batch_use_graph", c_int, [c_void_p, c_int]),
+    ("canoe_batch_step", c_int, [c_void_p]),
+    ("canoe_batch_synchronize", c_int, [c_void_p]),
+    ("canoe_batch_autotune", c_int, [c_void_p, c_void_p]),
     ("canoe_shell_create", c_int, [POINTER(ShellConfig), POINTER(c_void_p)]),
     ("canoe_shell_destroy", c_int, [c_void_p]),
     ("canoe_shell_dims", c_int, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32),

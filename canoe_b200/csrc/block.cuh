@@ -34,6 +34,9 @@ struct Geom {
   // cubed-sphere panel: device geometry tables (kShellTabs arrays of
   // nc3 * nc2 doubles, row-major [k][j]); null for a Cartesian block
   const double *shell;
+  // threads per x1 pencil (a multiple of 32 in 64..160; 0 = 160), chosen
+  // per block by canoe_batch_autotune
+  int col_threads;
 };
 
 // geometry tables of a cubed-sphere panel (gnomonic_equiangle.cpp:140-222)

@@ -609,4 +609,195 @@ int canoe_block_error_word(canoe_block_t b, uint32_t *bits) {
   return 0;
 }
 
+
+int canoe_block_set_column_threads(canoe_block_t b, int threads) {
+  if (!b) return CANOE_ERR_ARG;
+  if (threads != 0 && (threads < 64 || threads > kColThreads || threads % 32)) {
+    set_error("threads per x1 pencil must be a multiple of 32 in 64..160 (0: default)");
+    return CANOE_ERR_ARG;
+  }
+  b->g.col_threads = threads;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batches of uneven blocks: one step of every block as one graph whose
+// branches (one per block, on the block's stream) run concurrently
+
+struct canoe_batch {
+  std::vector<canoe_block *> blocks;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph = true;
+};
+
+static int batch_free(canoe_batch *q) {
+  if (!q) return 0;
+  if (q->gexec) cudaGraphExecDestroy(q->gexec);
+  for (cudaEvent_t e : q->join) cudaEventDestroy(e);
+  if (q->fork) cudaEventDestroy(q->fork);
+  if (q->st) cudaStreamDestroy(q->st);
+  delete q;
+  return 0;
+}
+
+// fork from the batch stream to every block stream, step, join
+static int batch_launches(canoe_batch *q) {
+  CB_CUDA(cudaEventRecord(q->fork, q->st));
+  for (size_t n = 0; n < q->blocks.size(); ++n) {
+    canoe_block *b = q->blocks[n];
+    CB_CUDA(cudaStreamWaitEvent(b->st, q->fork, 0));
+    if (int rc = step_launches(b, 0.)) return rc;
+    CB_CUDA(cudaEventRecord(q->join[n], b->st));
+    CB_CUDA(cudaStreamWaitEvent(q->st, q->join[n], 0));
+  }
+  return 0;
+}
+
+extern "C" {
+
+int canoe_batch_create(canoe_block_t *blocks, int n, canoe_batch_t *out) {
+  if (!blocks || n <= 0 || !out) {
+    set_error("canoe_batch_create: no blocks");
+    return CANOE_ERR_ARG;
+  }
+  canoe_batch *q = new canoe_batch();
+  for (int i = 0; i < n; ++i) {
+    if (!blocks[i]) {
+      batch_free(q);
+      set_error("canoe_batch_create: null block");
+      return CANOE_ERR_ARG;
+    }
+    q->blocks.push_back(blocks[i]);
+  }
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&q->st, cudaStreamNonBlocking)) ||
+      (e = cudaEventCreateWithFlags(&q->fork, cudaEventDisableTiming))) {
+    batch_free(q);
+    return cuda_status(e, "canoe_batch_create");
+  }
+  q->join.resize(n, nullptr);
+  for (int i = 0; i < n; ++i)
+    if ((e = cudaEventCreateWithFlags(&q->join[i], cudaEventDisableTiming))) {
+      batch_free(q);
+      return cuda_status(e, "canoe_batch_create");
+    }
+  *out = q;
+  return 0;
+}
+
+int canoe_batch_destroy(canoe_batch_t q) {
+  if (q && q->st) cudaStreamSynchronize(q->st);
+  return batch_free(q);
+}
+
+int canoe_batch_use_graph(canoe_batch_t q, int on) {
+  if (!q) return CANOE_ERR_ARG;
+  q->graph = on != 0;
+  if (q->gexec) {
+    cudaGraphExecDestroy(q->gexec);
+    q->gexec = nullptr;
+  }
+  return 0;
+}
+
+int canoe_batch_step(canoe_batch_t q) {
+  if (!q) return CANOE_ERR_ARG;
+  if (!q->graph) return batch_launches(q);
+  if (!q->gexec) {
+    cudaGraph_t graph;
+    CB_CUDA(cudaStreamBeginCapture(q->st, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_launches(q);
+    cudaError_t e = cudaStreamEndCapture(q->st, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&q->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+  }
+  CB_CUDA(cudaGraphLaunch(q->gexec, q->st));
+  return 0;
+}
+
+int canoe_batch_synchronize(canoe_batch_t q) {
+  if (!q) return CANOE_ERR_ARG;
+  CB_CUDA(cudaStreamSynchronize(q->st));
+  return 0;
+}
+
+// Per block, time steps with each candidate number of threads per x1
+// pencil (64, 96, 128, 160) and keep the fastest; the blocks' states, dt
+// and counters are restored afterwards.  h_threads (may be NULL) receives
+// the choices.
+int canoe_batch_autotune(canoe_batch_t q, int32_t *h_threads) {
+  if (!q) return CANOE_ERR_ARG;
+  static const int cand[4] = {64, 96, 128, 160};
+  cudaEvent_t e0, e1;
+  CB_CUDA(cudaEventCreate(&e0));
+  CB_CUDA(cudaEventCreate(&e1));
+  int rc = 0;
+  for (size_t n = 0; n < q->blocks.size() && !rc; ++n) {
+    canoe_block *b = q->blocks[n];
+    const size_t bytes = b->nvals * sizeof(double);
+    double *su = nullptr, *sw = nullptr, dts[2];
+    if (cudaMalloc(&su, bytes) || cudaMalloc(&sw, bytes)) {
+      rc = cuda_status(cudaErrorMemoryAllocation, "canoe_batch_autotune");
+      break;
+    }
+    cudaMemcpyAsync(su, b->d_u, bytes, cudaMemcpyDeviceToDevice, b->st);
+    cudaMemcpyAsync(sw, b->d_w, bytes, cudaMemcpyDeviceToDevice, b->st);
+    cudaMemcpyAsync(dts, b->d_dt, sizeof(dts), cudaMemcpyDeviceToHost, b->st);
+    cudaStreamSynchronize(b->st);
+    float best = 1e30f;
+    int pick = kColThreads;
+    for (int c : cand) {
+      b->g.col_threads = c;
+      if ((rc = step_launches(b, 0.))) break;
+      cudaEventRecord(e0, b->st);
+      for (int r = 0; r < 2 && !rc; ++r) rc = step_launches(b, 0.);
+      cudaEventRecord(e1, b->st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      // restore the state for the next candidate
+      cudaMemcpyAsync(b->d_u, su, bytes, cudaMemcpyDeviceToDevice, b->st);
+      cudaMemcpyAsync(b->d_w, sw, bytes, cudaMemcpyDeviceToDevice, b->st);
+      cudaMemcpyAsync(b->d_dt, dts, sizeof(dts), cudaMemcpyHostToDevice, b->st);
+      cudaStreamSynchronize(b->st);
+      if (rc) break;
+      if (ms < best) {
+        best = ms;
+        pick = c;
+      }
+    }
+    b->g.col_threads = pick;
+    if (b->gexec) {
+      cudaGraphExecDestroy(b->gexec);
+      b->gexec = nullptr;
+    }
+    cudaMemsetAsync(b->d_sat, 0, 4 * sizeof(unsigned long long), b->st);
+    cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), b->st);
+    cudaStreamSynchronize(b->st);
+    cudaFree(su);
+    cudaFree(sw);
+    if (h_threads) h_threads[n] = pick;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (q->gexec) {
+    cudaGraphExecDestroy(q->gexec);
+    q->gexec = nullptr;
+  }
+  if (!rc) CB_CUDA(cudaGetLastError());
+  return rc;
+}
+
 }  // extern "C"

@@ -732,6 +732,11 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
     return CANOE_ERR_UNSUPPORTED;
   }
   const unsigned nblk = (unsigned)g.nx2 * (unsigned)g.nx3;
+  // threads per pencil: the kernel strides every loop by blockDim and needs
+  // at least two warps (warp 0 runs the scan while the others reconstruct)
+  const int nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)
+                       ? g.col_threads
+                       : kColThreads;
   // bulk copies move whole pencil rows: 16-byte aligned bases and an even
   // row length keep every row 16-byte aligned
   auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };
@@ -739,7 +744,7 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
   gg.bulk = (g.nc1 % 2 == 0) && al16(w) && al16(du) && al16(u) && al16(u1) ? 1 : 0;
   auto go = [&](auto kern) -> int {
     if (int rc = ensure_smem((const void *)kern, smem)) return rc;
-    kern<<<nblk, kColThreads, smem, st>>>(gg, th, w, du, u, u1, dtp, s, stage, fout);
+    kern<<<nblk, nthr, smem, st>>>(gg, th, w, du, u, u1, dtp, s, stage, fout);
     CB_CUDA(cudaGetLastError());
     return 0;
   };

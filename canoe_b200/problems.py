@@ -304,3 +304,21 @@ def shell_c3(nx1=64, nside=96, p_bot=100.0e5, p_top=0.1e5, t1bar=165.0, radius=7
     cfg.cfl = cfl
     cfg.thermo = th
     return ShellProblem("C3-shell", cfg, x1f, u, w, dict(jet_amplitudes=amp, seed=seed))
+
+
+def batch_c5(nblocks=48, seed=20240605, nz=(32, 256), nh=(16, 128), depth=16.0e3, dx=250.0,
+             **kw):
+    """C5: nblocks independent blocks of C2 physics (moist3d: PPM + HLLC,
+    implicit x1, saturation adjustment) with vertical sizes nz and square
+    horizontal sizes nh drawn log-uniformly from the seed; every block is
+    depth deep with dx horizontal spacing.  Returns a list of Problems."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for b in range(nblocks):
+        n1 = int(round(np.exp(rng.uniform(np.log(nz[0]), np.log(nz[1])))))
+        n2 = int(round(np.exp(rng.uniform(np.log(nh[0]), np.log(nh[1])))))
+        p = moist3d(nx1=n1, nx2=n2, nx3=n2, x1max=depth, x2max=n2 * dx, x3max=n2 * dx,
+                    seed=seed + 1 + b, **kw)
+        p.name = f"C5-block{b}-{n1}x{n2}x{n2}"
+        out.append(p)
+    return out

@@ -141,6 +141,7 @@ typedef struct canoe_shell_config {
 } canoe_shell_config_t;
 
 typedef struct canoe_shell *canoe_shell_t;
+typedef struct canoe_batch *canoe_batch_t;
 
 /* ---------------- version / diagnostics ---------------- */
 const char *canoe_version(void);
@@ -323,6 +324,26 @@ int canoe_block_satadj_stats(canoe_block_t b, unsigned long long *h_stats);
 
 /* read and clear the block's device error word (canoe_errbit bits) */
 int canoe_block_error_word(canoe_block_t b, uint32_t *bits);
+
+/* Threads per x1 pencil (CTA of the column kernel): a multiple of 32 in
+ * 64..160, 0 for the default 160.  Results do not depend on it.  No
+ * reference counterpart (the reference sweeps columns serially). */
+int canoe_block_set_column_threads(canoe_block_t b, int threads);
+
+/* ---------------- batches of uneven blocks ----------------
+ * Steps many blocks as one CUDA graph whose branches (one per block, on the
+ * block's own stream) run concurrently; each block uses its own device dt
+ * (canoe_block_set_fixed_dt or its CFL step).  The reference steps its
+ * MeshBlocks one after another in the task list (TaskList::
+ * DoTaskListOneStage, called at main.cpp:119-121); no direct counterpart. */
+int canoe_batch_create(canoe_block_t *blocks, int n, canoe_batch_t *out);
+int canoe_batch_destroy(canoe_batch_t q);
+int canoe_batch_use_graph(canoe_batch_t q, int on);
+int canoe_batch_step(canoe_batch_t q);
+int canoe_batch_synchronize(canoe_batch_t q);
+/* pick the fastest threads per x1 pencil of every block by timing; the
+ * blocks' states are restored; h_threads[n] (may be NULL) gets the choices */
+int canoe_batch_autotune(canoe_batch_t q, int32_t *h_threads);
 
 /* ---------------- cubed-sphere shell (exo3) ----------------
  * All six panels resident on one GPU in one array (6, NV, nc3, nc2, nc1),
