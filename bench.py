@@ -129,6 +129,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
+def job_rates(ms_list, cells_per_rank, steps, dist=None, device="cuda"):
+    """Max over ranks of each timed region (ms, CUDA events) and the
+    whole-job zone-cycles/s: every rank advances its own replica of
+    cells_per_rank cells (weak scaling, no data-path collective)."""
+    import torch
+    t = torch.tensor(ms_list, dtype=torch.float64, device=device)
+    world = 1
+    if dist is not None and dist.is_initialized():
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        world = dist.get_world_size()
+    ms = [float(x) for x in t.tolist()]
+    return ms, [world * cells_per_rank * steps / (m * 1e-3) for m in ms]
+
+
 def make_problem(args, nx2=None, nx3=None):
     from canoe_b200 import problems
     return problems.moist3d(nx1=args.nx1, nx2=nx2 or args.nx2, nx3=nx3 or args.nx3,
@@ -471,14 +485,10 @@ def main():
         stream.synchronize()
     launches = args.steps * sum(LAUNCHES_PER_STEP.values())
     err = blk.error_word()
-    t = torch.tensor([results[args.precision]["ms"], results[order[1]]["ms"]], device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, ms_other = float(t[0].item()), float(t[1].item())
+    (ms, ms_other), (value, value_other) = job_rates(
+        [results[args.precision]["ms"], results[order[1]]["ms"]], ncell, args.steps, dist)
     ms_step = ms / args.steps
-    value = world * ncell * args.steps / (ms * 1e-3)
-    other = {"variant": order[1], "value": world * ncell * args.steps / (ms_other * 1e-3),
-             "ms_per_step": ms_other / args.steps}
+    other = {"variant": order[1], "value": value_other, "ms_per_step": ms_other / args.steps}
 
     # roofline of the dominant kernel class
     hbm, peak_kind = peaks()
