@@ -381,7 +381,19 @@ def main():
     ap.add_argument("--no-c4", action="store_true")
     ap.add_argument("--no-c3", action="store_true")
     ap.add_argument("--no-c5", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
+                    help="c2: the headline line; c3 / c5: only that report, as one JSON line")
     args = ap.parse_args()
+    if args.workload != "c2":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if args.workload == "c3":
+            rep = c3_report(steps=args.steps, warmup=args.warmup)
+        else:
+            from canoe_b200 import learned
+            rep = c5_report(learned.default_net(), steps=args.steps, warmup=args.warmup)
+        print(json.dumps({"workload": args.workload, **rep}), flush=True)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
