@@ -227,52 +227,66 @@ def c4_report(net, th, ncells=1 << 24):
 
 
 def c3_report(steps=10, warmup=3, nx1=64, nside=96, dt=60.0):
-    """C3: the six-panel cubed-sphere shell (FP64, PPM + HLLC, implicit x1)
-    stepped on device with the panel exchange; zone-cycles/s and the ghost
-    exchange's bandwidth (algorithmic bytes: two source reads and one write
-    of NV doubles per ghost cell)."""
+    """C3: the six-panel cubed-sphere shell (PPM + HLLC, implicit x1) stepped
+    on device with the panel exchange, FP32 fluxes on the hydrostatic
+    perturbation against plain FP64: zone-cycles/s of both, the L2 difference
+    after the same steps, and the ghost exchange's bandwidth (algorithmic
+    bytes: two source reads and one write of NV doubles per ghost cell)."""
     import torch
     from canoe_b200 import Shell, problems
     from canoe_b200._abi import check
-    p = problems.shell_c3(nx1=nx1, nside=nside)
-    sh = Shell(p)
-    stream = torch.cuda.Stream()
-    check(sh.lib.canoe_shell_set_stream(sh.h, ctypes.c_void_p(stream.cuda_stream)))
     cells = 6 * nside * nside * nx1
     out = {"cells": cells, "config": f"6 x {nside}x{nside} x {nx1}, PPM + HLLC, implicit x1 "
-           "partial 3x3, FP64 (the shell has no FP32 path)", "dt": dt}
-    with torch.cuda.stream(stream):
-        for _ in range(warmup):
-            sh.step(dt)
-        stream.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            sh.step(dt)
-        e1.record(stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        out["ms_per_step"] = ms / steps
-        out["value"] = cells * steps / (ms * 1e-3)
-        out["unit"] = UNIT
-        # the ghost exchange alone, repeated (its inputs are the panels'
-        # edge layers, 53 MB per call at full size: they stay in L2)
-        reps = 50
-        e0.record(stream)
-        for _ in range(reps):
-            check(sh.lib.canoe_shell_fill_ghosts(sh.h))
-        e1.record(stream)
-        e1.synchronize()
-        us = e0.elapsed_time(e1) * 1e3 / reps
-        ghosts = 6 * 4 * 3 * nside * nx1
-        byts = 3 * 8 * 5 * ghosts
-        out["ghost_exchange"] = {"us_per_call": us, "ghost_cells": ghosts,
-                                 "algorithmic_bytes": byts, "gbs": byts / (us * 1e-6) / 1e9,
-                                 "note": "repeated calls: source layers L2-resident"}
-    w = p.interior(sh.primitive())
-    out["finite"] = bool(np.isfinite(w).all())
-    out["error_word"] = sh.error_word()
-    sh.close()
+           "partial 3x3", "dt": dt, "unit": UNIT}
+    stream = torch.cuda.Stream()
+    states = {}
+    for name, prec in (("mixed", 1), ("fp64", 0)):
+        p = problems.shell_c3(nx1=nx1, nside=nside)
+        p.cfg.precision = prec
+        sh = Shell(p)
+        check(sh.lib.canoe_shell_set_stream(sh.h, ctypes.c_void_p(stream.cuda_stream)))
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                sh.step(dt)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                sh.step(dt)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            rec = {"ms_per_step": ms / steps, "value": cells * steps / (ms * 1e-3)}
+            if name == "fp64":
+                # the ghost exchange alone, repeated (its inputs, the panels'
+                # edge layers, 53 MB at full size, stay in L2)
+                reps = 50
+                e0.record(stream)
+                for _ in range(reps):
+                    check(sh.lib.canoe_shell_fill_ghosts(sh.h))
+                e1.record(stream)
+                e1.synchronize()
+                us = e0.elapsed_time(e1) * 1e3 / reps
+                ghosts = 6 * 4 * 3 * nside * nx1
+                byts = 3 * 8 * 5 * ghosts
+                out["ghost_exchange"] = {"us_per_call": us, "ghost_cells": ghosts,
+                                         "algorithmic_bytes": byts,
+                                         "gbs": byts / (us * 1e-6) / 1e9,
+                                         "note": "repeated calls: source layers L2-resident"}
+        states[name] = p.interior(sh.conserved())
+        rec["finite"] = bool(np.isfinite(states[name]).all())
+        rec["error_word"] = sh.error_word()
+        out[name] = rec
+        sh.close()
+    a, b = states["mixed"], states["fp64"]
+    out["l2_error_mixed_vs_fp64"] = {
+        "density": float(np.linalg.norm(a[:, 0] - b[:, 0]) / np.linalg.norm(b[:, 0])),
+        "momentum": float(np.linalg.norm(a[:, 1:4] - b[:, 1:4]) / np.linalg.norm(b[:, 1:4])),
+        "energy": float(np.linalg.norm(a[:, 4] - b[:, 4]) / np.linalg.norm(b[:, 4])),
+        "steps": warmup + steps}
+    out["value"] = out["mixed"]["value"]
+    out["ms_per_step"] = out["mixed"]["ms_per_step"]
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     return out
 
 

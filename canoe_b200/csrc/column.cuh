@@ -324,7 +324,10 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         }
       }
       if constexpr (GEO) {
-        hllc<R, NY, 0, true>(th, wl, wr, fx, R(tab(kTabCosC, k, j)));
+        if constexpr (PERT)
+          hllc_pert<R, NY, 0, true>(th, wl, wr, R(pf), fx, R(tab(kTabCosC, k, j)));
+        else
+          hllc<R, NY, 0, true>(th, wl, wr, fx, R(tab(kTabCosC, k, j)));
         const R cth = R(tab(kTabCth1, k, j));
         const R ty = fx[S::IVY], tz = fx[S::IVZ];
         fx[S::IVY] = ty + tz * cth;
@@ -388,8 +391,10 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       for (int n = 0; n < NV; ++n) {
         double v;
         if constexpr (GEO) {
-          const double dfl = a1p * (double)F[n * (nx1 + 1) + f0 + 1] -
-                             a1m * (double)F[n * (nx1 + 1) + f0];
+          double dfl = a1p * (double)F[n * (nx1 + 1) + f0 + 1] -
+                       a1m * (double)F[n * (nx1 + 1) + f0];
+          // FP32 path: the momentum flux lacks psf, whose divergence is FP64
+          if (PERT && n == S::IVX && grav != 0.) dfl += a1p * psf[i + 1] - a1m * psf[i];
           v = -(wght * dfl / vol);
           if (n == S::IVX) v += csrc[0];
           if (n == S::IVY) v += csrc[1];
@@ -750,7 +755,7 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
   };
   const bool ppm = recon == CANOE_RECON_PPM, hllc = rs == CANOE_RSOLVER_HLLC;
   if (g.shell) {  // cubed-sphere panel: dry, FP64, HLLC
-    if constexpr (NY == 0 && sizeof(R) == 8) {
+    if constexpr (NY == 0) {
       if (!hllc) {
         set_error("the cubed-sphere panel uses the HLLC solver");
         return CANOE_ERR_UNSUPPORTED;
@@ -767,7 +772,7 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
       return CB_GCOL(5, kColStep);
 #undef CB_GCOL
     } else {
-      set_error("the cubed-sphere panel is dry and FP64");
+      set_error("the cubed-sphere panel is dry");
       return CANOE_ERR_UNSUPPORTED;
     }
   }

@@ -443,10 +443,12 @@ __global__ void k_shell_c2p(const double *__restrict__ u, double *__restrict__ w
 }
 
 // interior-side face states of the panel edges, rotated into the receiving
-// panel's frame; lr layout [panel][edge][pos][n][i - is]
-template <int RECON>
+// panel's frame; lr layout [panel][edge][pos][n][i - is].  R = float: the
+// FP32 path, reconstructed on p' = p - pref(i) as its flux kernel does.
+template <int RECON, typename R>
 __global__ void k_shell_edges(const double *__restrict__ w, const EdgeRow *__restrict__ rows,
                               int nrows, Geom g, int64_t pvals, double *__restrict__ lr) {
+  constexpr bool PERT = sizeof(R) == 4;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)nrows * g.nx1) return;
   const EdgeRow r = rows[t / g.nx1];
@@ -464,42 +466,52 @@ __global__ void k_shell_edges(const double *__restrict__ w, const EdgeRow *__res
     c0 = (int64_t)k * g.sk + (int64_t)(g.js + r.spos) * g.nc1 + i;
     sd = g.sk;
   }
-  double v[kNV];
+  const double pref = PERT ? g.pref[i] : 0.;
+  R v[kNV];
 #pragma unroll
   for (int n = 0; n < kNV; ++n) {
     const double *q = s + n * g.sv + c0;
-    double wL, wR;
+    const double sh = (PERT && n == 4) ? pref : 0.;
+    R wL, wR;
     if constexpr (RECON == CANOE_RECON_PPM)
-      ppm_cell(q[-2 * sd], q[-sd], q[0], q[sd], q[2 * sd], wL, wR);
+      ppm_cell(R(q[-2 * sd] - sh), R(q[-sd] - sh), R(q[0] - sh), R(q[sd] - sh),
+               R(q[2 * sd] - sh), wL, wR);
     else
-      plm_cell(q[-sd], q[0], q[sd], wL, wR);
+      plm_cell(R(q[-sd] - sh), R(q[0] - sh), R(q[sd] - sh), wL, wR);
     v[n] = up ? wR : wL;
   }
-  const double vy = v[2], vz = v[3];
-  v[2] = r.m[0][0] * vy + r.m[0][1] * vz;
-  v[3] = r.m[1][0] * vy + r.m[1][1] * vz;
+  const R vy = v[2], vz = v[3];
+  v[2] = R(r.m[0][0]) * vy + R(r.m[0][1]) * vz;
+  v[3] = R(r.m[1][0]) * vy + R(r.m[1][1]) * vz;
   const int N = g.nx2;
   double *o = lr + ((((int64_t)r.dst * 4 + r.ddir) * N + r.dpos) * kNV) * g.nx1 + ii;
 #pragma unroll
-  for (int n = 0; n < kNV; ++n) o[(int64_t)n * g.nx1] = v[n];
+  for (int n = 0; n < kNV; ++n) o[(int64_t)n * g.nx1] = (double)v[n];
 }
 
 constexpr int TI = 32, TD = 8;
 
 // x2 (DIR 1) / x3 (DIR 2) fluxes and their divergence on (32 i) x (8 cells)
-// tiles; blockIdx.z runs over panel x rows
-template <int RECON, int DIR, bool WF>
+// tiles; blockIdx.z runs over panel x rows.  R = float: reconstruction and
+// the Riemann solver in FP32 on p' = p - pref(i); the metric transforms, the
+// projection and the divergence stay FP64, with pref added back to the
+// normal momentum flux before them (the transforms mix it into the
+// transverse components, and face areas differ across a cell).
+template <int RECON, int DIR, bool WF, typename R>
 __global__ void __launch_bounds__(256)
     k_shell_flux_x23(Geom g, canoe_thermo_t th, const double *__restrict__ w,
                      double *__restrict__ du, const double *__restrict__ dtp, double beta,
                      int64_t pvals, const double *__restrict__ lr, double *__restrict__ fout) {
   constexpr int QR = TD + 2 * NG, RR = TD + 2;
+  constexpr bool PERT = sizeof(R) == 4;
   extern __shared__ double sm_[];
-  double(*q)[QR][TI] = reinterpret_cast<double(*)[QR][TI]>(sm_);
-  double(*WL)[RR][TI] = reinterpret_cast<double(*)[RR][TI]>(sm_ + kNV * QR * TI);
-  double(*WR)[RR][TI] = reinterpret_cast<double(*)[RR][TI]>(sm_ + kNV * (QR + RR) * TI);
-  // F aliases q, which P1 is the last to read
-  double(*F)[TD + 1][TI] = reinterpret_cast<double(*)[TD + 1][TI]>(sm_);
+  R *smr = reinterpret_cast<R *>(sm_);
+  R(*q)[QR][TI] = reinterpret_cast<R(*)[QR][TI]>(smr);
+  R(*WL)[RR][TI] = reinterpret_cast<R(*)[RR][TI]>(smr + kNV * QR * TI);
+  R(*WR)[RR][TI] = reinterpret_cast<R(*)[RR][TI]>(smr + kNV * (QR + RR) * TI);
+  // FP64 fluxes: over q (FP64 path, P1 reads q last) or after WR (FP32)
+  double(*F)[TD + 1][TI] = reinterpret_cast<double(*)[TD + 1][TI]>(
+      PERT ? reinterpret_cast<double *>(smr + kNV * (QR + 2 * RR) * TI) : sm_);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i = g.is + blockIdx.x * TI + tx;
   const bool iok = i <= g.ie;
@@ -514,16 +526,21 @@ __global__ void __launch_bounds__(256)
   const int64_t pb = p * pvals;
   const int64_t base = (DIR == 1 ? (int64_t)o * g.sk : (int64_t)o * g.nc1) + i;
   const int64_t nkj = (int64_t)g.nc3 * g.nc2;
+  const double pref = PERT ? g.pref[iok ? i : g.is] : 0.;
   for (int c = ty; c < nd + 2 * NG; c += blockDim.y) {
     const int64_t off = pb + base + (int64_t)(d0 - NG + c) * sd;
 #pragma unroll
-    for (int n = 0; n < kNV; ++n) q[n][c][tx] = iok ? w[n * g.sv + off] : 1.;
+    for (int n = 0; n < kNV; ++n) {
+      double v = iok ? w[n * g.sv + off] : 1.;
+      if (PERT && n == 4) v = iok ? v - pref : 0.;
+      q[n][c][tx] = R(v);
+    }
   }
   __syncthreads();
   for (int c = ty; c < nd + 2; c += blockDim.y) {
 #pragma unroll
     for (int n = 0; n < kNV; ++n) {
-      double wl_, wr_;
+      R wl_, wr_;
       if constexpr (RECON == CANOE_RECON_PPM)
         ppm_cell(q[n][c][tx], q[n][c + 1][tx], q[n][c + 2][tx], q[n][c + 3][tx],
                  q[n][c + 4][tx], wl_, wr_);
@@ -536,7 +553,8 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   for (int f = ty; f <= nd; f += blockDim.y) {
     const int fd = d0 + f;
-    double wl[kNV], wr[kNV], fx[kNV];
+    R wl[kNV], wr[kNV], fr[kNV];
+    double fx[kNV];
 #pragma unroll
     for (int n = 0; n < kNV; ++n) {
       wl[n] = WR[n][f][tx];
@@ -548,13 +566,13 @@ __global__ void __launch_bounds__(256)
       const double *s = lr + ((((int64_t)p * 4 + (DIR == 1 ? 0 : 2)) * N + pos) * kNV) * g.nx1 +
                         (i - g.is);
 #pragma unroll
-      for (int n = 0; n < kNV; ++n) wl[n] = s[(int64_t)n * g.nx1];
+      for (int n = 0; n < kNV; ++n) wl[n] = R(s[(int64_t)n * g.nx1]);
     }
     if (iok && fd == dhi + 1) {
       const double *s = lr + ((((int64_t)p * 4 + (DIR == 1 ? 1 : 3)) * N + pos) * kNV) * g.nx1 +
                         (i - g.is);
 #pragma unroll
-      for (int n = 0; n < kNV; ++n) wr[n] = s[(int64_t)n * g.nx1];
+      for (int n = 0; n < kNV; ++n) wr[n] = R(s[(int64_t)n * g.nx1]);
     }
     const int kf = DIR == 1 ? o : fd, jf = DIR == 1 ? fd : o;
     const int64_t kj = (int64_t)kf * g.nc2 + jf;
@@ -563,14 +581,20 @@ __global__ void __launch_bounds__(256)
       const double ct = g.shell[kTabCosF2 * nkj + kj], st = g.shell[kTabSinF2 * nkj + kj];
       const double gi22 = 1.0 / (st * st);
       const double T22 = 1.0 / sqrt(gi22), T32 = ct / sqrt(1.0), T33 = sqrt(1.0);
-      auto loc = [&](double *x) {
-        const double u2 = x[2], u3 = x[3];
-        x[2] = T22 * u2;
-        x[3] = T32 * u2 + T33 * u3;
+      auto loc = [&](R *x) {
+        const R u2 = x[2], u3 = x[3];
+        x[2] = R(T22) * u2;
+        x[3] = R(T32) * u2 + R(T33) * u3;
       };
       loc(wl);
       loc(wr);
-      hllc<double, 0, 1>(th, wl, wr, fx);
+      if constexpr (PERT)
+        hllc_pert<R, 0, 1>(th, wl, wr, R(pref), fr);
+      else
+        hllc<R, 0, 1>(th, wl, wr, fr);
+#pragma unroll
+      for (int n = 0; n < kNV; ++n) fx[n] = fr[n];
+      if (PERT) fx[2] += pref;
       const double F22 = sqrt(gi22), F32 = -sqrt(gi22) * ct / 1.0, F33 = 1.0 / sqrt(1.0);
       const double txy = fx[2], txz = fx[3];
       fx[2] = F22 * txy;
@@ -585,14 +609,20 @@ __global__ void __launch_bounds__(256)
       const double ct = g.shell[kTabCosF3 * nkj + kj], st = g.shell[kTabSinF3 * nkj + kj];
       const double gi33 = 1.0 / (st * st);
       const double T22 = sqrt(1.0), T23 = ct / sqrt(1.0), T33 = 1.0 / sqrt(gi33);
-      auto loc = [&](double *x) {
-        const double u2 = x[2], u3 = x[3];
-        x[2] = T22 * u2 + T23 * u3;
-        x[3] = T33 * u3;
+      auto loc = [&](R *x) {
+        const R u2 = x[2], u3 = x[3];
+        x[2] = R(T22) * u2 + R(T23) * u3;
+        x[3] = R(T33) * u3;
       };
       loc(wl);
       loc(wr);
-      hllc<double, 0, 2>(th, wl, wr, fx);
+      if constexpr (PERT)
+        hllc_pert<R, 0, 2>(th, wl, wr, R(pref), fr);
+      else
+        hllc<R, 0, 2>(th, wl, wr, fr);
+#pragma unroll
+      for (int n = 0; n < kNV; ++n) fx[n] = fr[n];
+      if (PERT) fx[3] += pref;
       const double F22 = 1.0 / sqrt(1.0), F23 = -ct / 1.0 * sqrt(gi33), F33 = sqrt(gi33);
       const double txy = fx[2], txz = fx[3];
       fx[2] = F22 * txy + F23 * txz;
@@ -661,7 +691,7 @@ struct canoe_shell {
   int64_t pvals = 0;  // values per panel
   double *d_u = nullptr, *d_w = nullptr, *d_u1 = nullptr, *d_du = nullptr;
   double *d_x1f = nullptr, *d_x1v = nullptr, *d_dx1f = nullptr, *d_dt = nullptr;
-  double *d_tabs = nullptr, *d_lr = nullptr;
+  double *d_tabs = nullptr, *d_lr = nullptr, *d_pref = nullptr;
   unsigned long long *d_dtacc = nullptr;
   uint32_t *d_err = nullptr;
   GhostRow *d_ghost = nullptr;
@@ -675,7 +705,8 @@ static int shell_free(canoe_shell *s) {
   if (!s) return 0;
   for (void *p : {(void *)s->d_u, (void *)s->d_w, (void *)s->d_u1, (void *)s->d_du,
                   (void *)s->d_x1f, (void *)s->d_x1v, (void *)s->d_dx1f, (void *)s->d_dt,
-                  (void *)s->d_tabs, (void *)s->d_lr, (void *)s->d_dtacc, (void *)s->d_err,
+                  (void *)s->d_tabs, (void *)s->d_lr, (void *)s->d_pref, (void *)s->d_dtacc,
+                  (void *)s->d_err,
                   (void *)s->d_ghost, (void *)s->d_edge})
     if (p) cudaFree(p);
   if (s->own_stream && s->st) cudaStreamDestroy(s->st);
@@ -703,24 +734,29 @@ static int shell_c2p(canoe_shell *s) {
 static int shell_edges(canoe_shell *s) {
   const int64_t n = (int64_t)s->nedge * s->g.nx1;
   const unsigned nb = (unsigned)((n + 255) / 256);
-  if (s->cfg.recon == CANOE_RECON_PPM)
-    k_shell_edges<CANOE_RECON_PPM><<<nb, 256, 0, s->st>>>(s->d_w, s->d_edge, s->nedge, s->g,
-                                                          s->pvals, s->d_lr);
-  else
-    k_shell_edges<CANOE_RECON_PLM><<<nb, 256, 0, s->st>>>(s->d_w, s->d_edge, s->nedge, s->g,
-                                                          s->pvals, s->d_lr);
+  const bool f32 = s->cfg.precision == CANOE_FP32_PERTURBATION;
+#define CB_SE(RC, R) \
+  k_shell_edges<RC, R><<<nb, 256, 0, s->st>>>(s->d_w, s->d_edge, s->nedge, s->g, s->pvals, s->d_lr)
+  if (s->cfg.recon == CANOE_RECON_PPM) {
+    if (f32) CB_SE(CANOE_RECON_PPM, float); else CB_SE(CANOE_RECON_PPM, double);
+  } else {
+    if (f32) CB_SE(CANOE_RECON_PLM, float); else CB_SE(CANOE_RECON_PLM, double);
+  }
+#undef CB_SE
   CB_CUDA(cudaGetLastError());
   return 0;
 }
 
-static int shell_x23(canoe_shell *s, int dir, double beta, double *fout) {
+template <typename R>
+static int shell_x23_t(canoe_shell *s, int dir, double beta, double *fout) {
   const Geom &g = s->g;
   dim3 grid((g.nx1 + TI - 1) / TI, (g.nx2 + TD - 1) / TD, 6 * g.nx2);
   dim3 blk(TI, 8);
-  const size_t smem = sizeof(double) * kNV * TI * ((TD + 2 * NG) + 2 * (TD + 2));
-#define CB_SX(R, D, W)                                                                           \
-  k_shell_flux_x23<R, D, W><<<grid, blk, smem, s->st>>>(g, s->th, s->d_w, s->d_du, s->d_dt, beta, \
-                                                        s->pvals, s->d_lr, fout)
+  const size_t tiles = sizeof(R) * kNV * TI * ((TD + 2 * NG) + 2 * (TD + 2));
+  const size_t smem = sizeof(R) == 8 ? tiles : tiles + sizeof(double) * kNV * (TD + 1) * TI;
+#define CB_SX(RC, D, W)                                                                   \
+  k_shell_flux_x23<RC, D, W, R><<<grid, blk, smem, s->st>>>(g, s->th, s->d_w, s->d_du,    \
+                                                            s->d_dt, beta, s->pvals, s->d_lr, fout)
   const bool ppm = s->cfg.recon == CANOE_RECON_PPM;
   if (dir == 1) {
     if (ppm) { if (fout) CB_SX(3, 1, true); else CB_SX(3, 1, false); }
@@ -732,6 +768,11 @@ static int shell_x23(canoe_shell *s, int dir, double beta, double *fout) {
 #undef CB_SX
   CB_CUDA(cudaGetLastError());
   return 0;
+}
+
+static int shell_x23(canoe_shell *s, int dir, double beta, double *fout) {
+  if (s->cfg.precision == CANOE_FP32_PERTURBATION) return shell_x23_t<float>(s, dir, beta, fout);
+  return shell_x23_t<double>(s, dir, beta, fout);
 }
 
 extern "C" {
@@ -746,8 +787,8 @@ int canoe_shell_create(const canoe_shell_config_t *cfg, canoe_shell_t *out) {
     return CANOE_ERR_ARG;
   }
   if (cfg->thermo.ny != 0 || cfg->rsolver != CANOE_RSOLVER_HLLC ||
-      cfg->precision != CANOE_FP64) {
-    set_error("canoe_shell_create: the cubed-sphere path is dry (ny = 0), HLLC and FP64");
+      (cfg->precision != CANOE_FP64 && cfg->precision != CANOE_FP32_PERTURBATION)) {
+    set_error("canoe_shell_create: the cubed-sphere path is dry (ny = 0) and HLLC");
     return CANOE_ERR_UNSUPPORTED;
   }
   if (cfg->bc_x1[0] == CANOE_BC_PERIODIC || cfg->bc_x1[1] == CANOE_BC_PERIODIC) {
@@ -810,6 +851,8 @@ int canoe_shell_create(const canoe_shell_config_t *cfg, canoe_shell_t *out) {
   if ((e = cudaMalloc(&s->d_x1v, xv.size() * sizeof(double)))) return fail(e, "cudaMalloc x1v");
   if ((e = cudaMalloc(&s->d_dx1f, dx.size() * sizeof(double)))) return fail(e, "cudaMalloc dx1f");
   if ((e = cudaMalloc(&s->d_dt, 2 * sizeof(double)))) return fail(e, "cudaMalloc dt");
+  if ((e = cudaMalloc(&s->d_pref, g.nc1 * sizeof(double)))) return fail(e, "cudaMalloc pref");
+  if ((e = cudaMemset(s->d_pref, 0, g.nc1 * sizeof(double)))) return fail(e, "cudaMemset pref");
   if ((e = cudaMalloc(&s->d_dtacc, sizeof(unsigned long long)))) return fail(e, "cudaMalloc acc");
   if ((e = cudaMalloc(&s->d_err, sizeof(uint32_t)))) return fail(e, "cudaMalloc err");
   if ((e = cudaMalloc(&s->d_tabs, tabs.size() * sizeof(double)))) return fail(e, "cudaMalloc tabs");
@@ -837,7 +880,7 @@ int canoe_shell_create(const canoe_shell_config_t *cfg, canoe_shell_t *out) {
   g.x1f = s->d_x1f;
   g.x1v = s->d_x1v;
   g.dx1f = s->d_dx1f;
-  g.pref = nullptr;
+  g.pref = s->d_pref;
   g.err = s->d_err;
   g.shell = s->d_tabs;
   *out = s;
@@ -874,6 +917,9 @@ int canoe_shell_set_conserved(canoe_shell_t s, const double *h_u, int fill) {
   if (fill) {
     if (int rc = shell_ghosts(s)) return rc;
     if (int rc = shell_c2p(s)) return rc;
+    // reference pressure of the FP32 flux path: the level mean of panel 0
+    // (every panel holds the same radial levels)
+    if (int rc = launch_level_mean_pressure(s->g, 0, s->d_w, s->d_pref, s->st)) return rc;
   }
   CB_CUDA(cudaStreamSynchronize(s->st));
   return 0;
@@ -907,7 +953,7 @@ int canoe_shell_calculate_fluxes(canoe_shell_t s, double *d_f1, double *d_f2, do
   if (d_f1) {
     const int64_t fvals = (int64_t)kNV * g.nc3 * g.nc2 * (g.nc1 + 1);
     for (int p = 0; p < 6; ++p)
-      if (int rc = launch_x1col(g, s->th, s->cfg.recon, s->cfg.rsolver, 0, CANOE_FP64,
+      if (int rc = launch_x1col(g, s->th, s->cfg.recon, s->cfg.rsolver, 0, s->cfg.precision,
                                 kColFluxOnly, s->d_w + p * s->pvals, s->d_du + p * s->pvals,
                                 s->d_u + p * s->pvals, s->d_u1 + p * s->pvals, s->d_dt,
                                 kRK3[0], 0, d_f1 + p * fvals, s->st))
@@ -931,7 +977,8 @@ int canoe_shell_step(canoe_shell_t s, double dt) {
     if ((rc = shell_x23(s, 2, sg.beta, nullptr))) return rc;
     for (int p = 0; p < 6; ++p)
       if ((rc = launch_x1col(s->g, s->th, s->cfg.recon, s->cfg.rsolver, s->cfg.implicit_flag,
-                             CANOE_FP64, kColStep, s->d_w + p * s->pvals, s->d_du + p * s->pvals,
+                             s->cfg.precision, kColStep, s->d_w + p * s->pvals,
+                             s->d_du + p * s->pvals,
                              s->d_u + p * s->pvals, s->d_u1 + p * s->pvals, s->d_dt, sg, stage,
                              nullptr, s->st)))
         return rc;

@@ -324,9 +324,11 @@ __device__ __forceinline__ void lmars_pert(const canoe_thermo_t &th, const R *wl
   flx[ipr] = ubar * ws[0] * h;
 }
 
-template <typename R, int NY, int DIR>
+// COVKE: the covariant kinetic energy of the x1 problem on a cubed-sphere
+// panel, as in hllc()
+template <typename R, int NY, int DIR, bool COVKE = false>
 __device__ __forceinline__ void hllc_pert(const canoe_thermo_t &th, const R *wl, const R *wr,
-                                          R pref, R *flx) {
+                                          R pref, R *flx, R ke_cth = R(0)) {
   using S = Slots<NY>;
   constexpr int IVX = S::IVX, IVY = S::IVY, IVZ = S::IVZ, IPR = S::IPR;
   constexpr int ivx = IVX + DIR;
@@ -354,8 +356,17 @@ __device__ __forceinline__ void hllc_pert(const canoe_thermo_t &th, const R *wl,
   R kappar = R(1) / (gammar - R(1));
   R cl = sqrt(gammal * pl / wli[0]);
   R cr = sqrt(gammar * pr / wri[0]);
-  R KE_l = R(0.5) * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * wli[IVY] + wli[IVZ] * wli[IVZ]);
-  R KE_r = R(0.5) * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * wri[IVY] + wri[IVZ] * wri[IVZ]);
+  R KE_l, KE_r;
+  if constexpr (COVKE) {
+    R vy = wli[IVY] + wli[IVZ] * ke_cth, vz = wli[IVZ] + wli[IVY] * ke_cth;
+    KE_l = R(0.5) * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * vy + wli[IVZ] * vz);
+    vy = wri[IVY] + wri[IVZ] * ke_cth;
+    vz = wri[IVZ] + wri[IVY] * ke_cth;
+    KE_r = R(0.5) * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * vy + wri[IVZ] * vz);
+  } else {
+    KE_l = R(0.5) * wli[0] * (wli[IVX] * wli[IVX] + wli[IVY] * wli[IVY] + wli[IVZ] * wli[IVZ]);
+    KE_r = R(0.5) * wri[0] * (wri[IVX] * wri[IVX] + wri[IVY] * wri[IVY] + wri[IVZ] * wri[IVZ]);
+  }
   R el = pl * kappal + KE_l;
   R er = pr * kappar + KE_r;
   R rhoa = R(.5) * (wli[0] + wri[0]);

@@ -94,3 +94,42 @@ def test_step_matches_oracle(oracle_mod, implicit_flag):
     m0 = sum((p.interior(p.u)[q, 0] * vol).sum() for q in range(6))
     m1 = sum((a[q, 0] * vol).sum() for q in range(6))
     assert abs(m1 - m0) / m0 < 1e-14
+
+
+def _c3_pair():
+    p64 = problems.shell_c3(nx1=16, nside=8)
+    p32 = problems.shell_c3(nx1=16, nside=8)
+    p32.cfg.precision = 1  # FP32 fluxes on the hydrostatic perturbation
+    return p64, p32
+
+
+def test_fp32_shell_fluxes_near_fp64():
+    p64, p32 = _c3_pair()
+    a = Shell(p64).calculate_fluxes()
+    b = Shell(p32).calculate_fluxes()
+    N, nx1 = p64.cfg.nside, p64.cfg.nx1
+    i, jk, fj = slice(NG, NG + nx1), slice(NG, NG + N), slice(NG, NG + N + 1)
+    sel = [(slice(None), slice(None), jk, jk, slice(NG, NG + nx1 + 1)),
+           (slice(None), slice(None), jk, fj, i), (slice(None), slice(None), fj, jk, i)]
+    for d in range(3):
+        print("flux", d + 1, rel_l2(b[d][sel[d]], a[d][sel[d]]))
+        assert rel_l2(b[d][sel[d]], a[d][sel[d]]) < 1e-5, d
+
+
+def test_fp32_shell_steps_near_fp64():
+    p64, p32 = _c3_pair()
+    s64, s32 = Shell(p64), Shell(p32)
+    for _ in range(5):
+        s64.step(5.0)
+        s32.step(5.0)
+    s64.synchronize()
+    s32.synchronize()
+    assert s32.error_word() == 0
+    a, b = p64.interior(s64.conserved()), p64.interior(s32.conserved())
+    errs = [rel_l2(b[:, n], a[:, n]) for n in range(5)]
+    print("state", errs)
+    assert max(errs) < 1e-6, errs
+    vol = cell_volumes(p64)
+    m0 = sum((a[q, 0] * vol).sum() for q in range(6))
+    m1 = sum((b[q, 0] * vol).sum() for q in range(6))
+    assert abs(m1 - m0) / m0 < 1e-12
