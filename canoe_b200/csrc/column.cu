@@ -20,8 +20,15 @@ int launch_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int
                  const double *dtp, const Stage &s, int stage, double *fo,
                  cudaStream_t st) {
   if ((flag & 1) && mode != kColFluxOnly && g.bc[0] == CANOE_BC_PERIODIC) {
-    set_error("implicit X1 solve with periodic x1 boundaries is not supported");
-    return CANOE_ERR_UNSUPPORTED;
+    // the cyclic solve couples the two ends (periodic_forward_backward.hpp)
+    if (g.bc[1] != CANOE_BC_PERIODIC) {
+      set_error("periodic x1 needs both x1 boundaries periodic");
+      return CANOE_ERR_ARG;
+    }
+    if (g.nx1 < 3) {
+      set_error("the periodic implicit x1 solve needs at least 3 levels");
+      return CANOE_ERR_ARG;
+    }
   }
   switch (th.ny) {
     case 0: return run_x1col<0>(g, th, recon, rs, flag, prec, mode, w, du, u, u1, dtp, s, stage, fo, st);

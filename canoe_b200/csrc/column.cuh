@@ -18,7 +18,11 @@
 //      and flux Jacobians of the cells are built once and shared
 //  P6  the block-tridiagonal solve by block cyclic reduction across the CTA
 //      (the reference eliminates sequentially, forward_backward.hpp:15-137;
-//      both solve the same system)
+//      both solve the same system).  Periodic x1 (PER): the cyclic system of
+//      periodic_forward_backward.hpp:15-234 is solved by bordering: the
+//      reduction runs on rows 0..n-2 with N extra right-hand columns (the
+//      couplings of rows 0 and n-2 to row n-1), then row n-1 closes with one
+//      N x N Schur-complement solve
 //  P7  forward_backward.hpp:101-124 species correction and the register
 //      update u = g1 u + g2 u1 + du (implicit_hydro_tasks.cpp:152-160, 283)
 // Every global access is contiguous along the pencil.
@@ -45,12 +49,12 @@ struct ColRow {
 
 // shared-memory plan (doubles) of one pencil
 struct ColSmem {
-  int wp, dc, uni, stg, mbar, total;
+  int wp, dc, uni, stg, z, mbar, total;
 };
 
 __host__ __device__ inline int even_up(int x) { return (x + 1) & ~1; }
 
-__host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl) {
+__host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl, int per = 0) {
   ColSmem s;
   s.wp = 0;                  // [NV][nc1] pristine pencil
   s.dc = nv * nc1;           // [NV][nc1] du of the column (interior at is)
@@ -58,6 +62,7 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
   const int flux = 3 * nv * nc1 + 3 * nc1 + 1;
   int solve = 0;
   s.stg = 0;
+  s.z = 0;
   if (n_impl) {
     const int nn = n_impl * n_impl;
     const int rows = even_up(nx1 * ((3 * nn + n_impl) | 1));
@@ -66,6 +71,10 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
     const int st = 2 * nv * nc1;
     s.stg = s.uni + rows;
     solve = rows + (aj > st ? aj : st);
+    if (per) {  // [nx1][nn] bordering columns of the periodic solve
+      s.z = s.uni + solve;
+      solve += nx1 * nn;
+    }
   }
   s.mbar = s.uni + even_up(flux > solve ? flux : solve);
   s.total = s.mbar + 4;  // 3 mbarriers, 8 bytes each
@@ -87,7 +96,11 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
 // (gnomonic_equiangle.cpp:224-432), the coordinate source terms
 // (AddCoordTermsDivergence, :833-878) and the implicit solve on velocities
 // projected to the local frame (solve_implicit_3d.cpp:105-137).
-template <int NY, int RECON, int RS, int N, int MODE, typename R, int GEO = 0>
+//
+// PER: periodic x1 (both ends), implicit modes only; the cyclic solve and the
+// reference's periodic du update without the species correction
+// (periodic_forward_backward.hpp:207-225).
+template <int NY, int RECON, int RS, int N, int MODE, typename R, int GEO = 0, bool PER = false>
 __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     k_x1col(Geom g, canoe_thermo_t th, const double *__restrict__ w,
             double *__restrict__ du, double *__restrict__ u, double *__restrict__ u1,
@@ -97,7 +110,7 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
   constexpr int NV = S::NV;
   extern __shared__ double sm[];
   const int nc1 = g.nc1, is = g.is, ie = g.ie, nx1 = g.nx1;
-  const ColSmem L = col_smem(NV, nc1, nx1, N);
+  const ColSmem L = col_smem(NV, nc1, nx1, N, PER);
   double *wp = sm + L.wp;
   double *dc = sm + L.dc;
   double *un = sm + L.uni;
@@ -491,6 +504,12 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     // of the last row couple to ghosts: the reflecting condition folds them
     // into a, and the sweep never uses them, so they are zeroed here.  Rows
     // that the first reduction level eliminates (r even) keep a^-1.
+    // PER: the reduction covers rows 0..nr-1 = n-2; b of row 0 (the upper
+    // corner, coupling to row n-1) and c of row n-2 move into the bordering
+    // columns Z, and row n-1 keeps a, b and, in place of c, the lower corner:
+    // c of the ghost row is-1 (periodic_forward_backward.hpp:67-72).
+    const int nr = PER ? nx1 - 1 : nx1;
+    double *zb = sm + L.z;  // PER: [nr][NN]
     for (int r = tid; r < nx1; r += nth) {
       const int i = is + r;
       double aL = area, aR = area;
@@ -514,13 +533,25 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         double a = (Am * aL + Ap * aR + (aR - aL) * Jc) * i2v + (rr == qq ? idt : 0.) - phi;
         const double b = -(Am + Jm) * aL * i2v;
         const double c = -(Ap - Jn) * aR * i2v;
-        if (i == is) a += (qq == 1 ? -b : b);
-        if (i == ie) a += (qq == 1 ? -c : c);
-        am.a[rr][qq] = a;
-        row[NN + e] = i == is ? 0. : b;
-        row[2 * NN + e] = i == ie ? 0. : c;
+        if constexpr (PER) {
+          am.a[rr][qq] = a;
+          row[NN + e] = r == 0 ? 0. : b;
+          if (r == nx1 - 1) {  // lower corner: c of row is-1
+            const double i2g = 1. / (2. * (g.dx1f[is - 1] * g.dx2 * g.dx3));
+            row[2 * NN + e] = -(sA[e] - sJ[NN + e]) * area * i2g;
+          } else {
+            row[2 * NN + e] = r == nr - 1 ? 0. : c;
+            zb[r * NN + e] = (r == 0 ? b : 0.) + (r == nr - 1 ? c : 0.);
+          }
+        } else {
+          if (i == is) a += (qq == 1 ? -b : b);
+          if (i == ie) a += (qq == 1 ? -c : c);
+          am.a[rr][qq] = a;
+          row[NN + e] = i == is ? 0. : b;
+          row[2 * NN + e] = i == ie ? 0. : c;
+        }
       }
-      stm(row, ((r & 1) == 0 && 1 < nx1) ? inv(am) : am);
+      stm(row, ((r & 1) == 0 && 1 < nr && r < nr) ? inv(am) : am);
       // right-hand side (forward_backward.hpp:24-41)
       double r0 = dc[i];
 #pragma unroll
@@ -571,7 +602,14 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       for (int e = 0; e < N; ++e) rh.a[e] += tv.a[e];
       M<N> bn = mm(al, ld(lo + NN));
       M<N> cn;
-      if (r + s < nx1) {
+      M<N> zr;
+      if constexpr (PER) {
+        zr = ld(zb + r * NN);
+        t = mm(al, ld(zb + (r - s) * NN));
+#pragma unroll
+        for (int e = 0; e < NN; ++e) zr.a[e / N][e % N] += t.a[e / N][e % N];
+      }
+      if (r + s < nr) {
         const double *hi = blk + (r + s) * ROW;
         M<N> ga = mm(c, ld(hi));
 #pragma unroll
@@ -583,47 +621,69 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
 #pragma unroll
         for (int e = 0; e < N; ++e) rh.a[e] += tv.a[e];
         cn = mm(ga, ld(hi + 2 * NN));
+        if constexpr (PER) {
+          t = mm(ga, ld(zb + (r + s) * NN));
+#pragma unroll
+          for (int e = 0; e < NN; ++e) zr.a[e / N][e % N] += t.a[e / N][e % N];
+        }
       } else {
 #pragma unroll
         for (int e = 0; e < NN; ++e) cn.a[e / N][e % N] = 0.;
       }
-      const bool next_elim = (m & 1) == 0 && 4 * s - 1 < nx1;
+      const bool next_elim = (m & 1) == 0 && 4 * s - 1 < nr;
       stm(row, next_elim ? inv(a) : a);
       stm(row + NN, bn);
       stm(row + 2 * NN, cn);
       stv(row + 3 * NN, rh);
+      if constexpr (PER) stm(zb + r * NN, zr);
     };
     auto back = [&](int s, int m) {
       const int r = s - 1 + 2 * s * m;
       double *row = blk + r * ROW;
       V<N> rh = ldv(row + 3 * NN);
+      M<N> zr;
+      if constexpr (PER) zr = ld(zb + r * NN);
       if (r - s >= 0) {
-        V<N> t = mv(ld(row + NN), ldv(blk + (r - s) * ROW + 3 * NN));
+        const M<N> bm = ld(row + NN);
+        V<N> t = mv(bm, ldv(blk + (r - s) * ROW + 3 * NN));
 #pragma unroll
         for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
+        if constexpr (PER) {
+          const M<N> tz = mm(bm, ld(zb + (r - s) * NN));
+#pragma unroll
+          for (int e = 0; e < NN; ++e) zr.a[e / N][e % N] -= tz.a[e / N][e % N];
+        }
       }
-      if (r + s < nx1) {
-        V<N> t = mv(ld(row + 2 * NN), ldv(blk + (r + s) * ROW + 3 * NN));
+      if (r + s < nr) {
+        const M<N> cm = ld(row + 2 * NN);
+        V<N> t = mv(cm, ldv(blk + (r + s) * ROW + 3 * NN));
 #pragma unroll
         for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
+        if constexpr (PER) {
+          const M<N> tz = mm(cm, ld(zb + (r + s) * NN));
+#pragma unroll
+          for (int e = 0; e < NN; ++e) zr.a[e / N][e % N] -= tz.a[e / N][e % N];
+        }
       }
-      stv(row + 3 * NN, mv(ld(row), rh));
+      const M<N> ai = ld(row);
+      stv(row + 3 * NN, mv(ai, rh));
+      if constexpr (PER) stm(zb + r * NN, mm(ai, zr));
     };
-    int stop = 1;  // first s with 2 s - 1 >= nx1
-    while (2 * stop - 1 < nx1) stop *= 2;
+    int stop = 1;  // first s with 2 s - 1 >= nr
+    while (2 * stop - 1 < nr) stop *= 2;
     int s = 1;
-    for (; s < stop && nx1 / (2 * s) > 32; s *= 2) {
-      for (int m = tid; m < nx1 / (2 * s); m += nth) level(s, m);
+    for (; s < stop && nr / (2 * s) > 32; s *= 2) {
+      for (int m = tid; m < nr / (2 * s); m += nth) level(s, m);
       __syncthreads();
     }
     const int s_warp = s;  // first level done by warp 0
     // first back level done by all threads: the largest s with > 32 rows
     int sb = 1;
-    while (2 * sb < stop && (nx1 + 2 * sb) / (4 * sb) > 32) sb *= 2;
-    if ((nx1 + sb) / (2 * sb) <= 32) sb = 0;  // every back level fits in warp 0
+    while (2 * sb < stop && (nr + 2 * sb) / (4 * sb) > 32) sb *= 2;
+    if ((nr + sb) / (2 * sb) <= 32) sb = 0;  // every back level fits in warp 0
     if (warp == 0) {
       for (s = s_warp; s < stop; s *= 2) {
-        for (int m = lane; m < nx1 / (2 * s); m += 32) level(s, m);
+        for (int m = lane; m < nr / (2 * s); m += 32) level(s, m);
         __syncwarp();
       }
       // the last surviving row r = stop - 1 is decoupled
@@ -632,16 +692,43 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
         M<N> ai = inv(ld(row));
         stm(row, ai);
         stv(row + 3 * NN, mv(ai, ldv(row + 3 * NN)));
+        if constexpr (PER) stm(zb + (stop - 1) * NN, mm(ai, ld(zb + (stop - 1) * NN)));
       }
       __syncwarp();
       for (s = stop / 2; s >= 1 && s > sb; s /= 2) {
-        for (int m = lane; m < (nx1 + s) / (2 * s); m += 32) back(s, m);
+        for (int m = lane; m < (nr + s) / (2 * s); m += 32) back(s, m);
         __syncwarp();
       }
     }
     __syncthreads();
     for (s = sb; s >= 1; s /= 2) {
-      for (int m = tid; m < (nx1 + s) / (2 * s); m += nth) back(s, m);
+      for (int m = tid; m < (nr + s) / (2 * s); m += nth) back(s, m);
+      __syncthreads();
+    }
+    if constexpr (PER) {
+      // rows 0..n-2 hold y and Z with x = y - Z x(n-1); row n-1:
+      // (a - s Z0 - b Z(n-2)) x(n-1) = rhs - s y0 - b y(n-2)
+      if (tid == 0) {
+        double *row = blk + (nx1 - 1) * ROW;
+        const M<N> bl = ld(row + NN), sc = ld(row + 2 * NN);
+        M<N> sch = ld(row);
+        V<N> rh = ldv(row + 3 * NN);
+        const M<N> t0 = mm(sc, ld(zb)), t1 = mm(bl, ld(zb + (nr - 1) * NN));
+        const V<N> v0 = mv(sc, ldv(blk + 3 * NN)), v1 = mv(bl, ldv(blk + (nr - 1) * ROW + 3 * NN));
+#pragma unroll
+        for (int e = 0; e < NN; ++e) sch.a[e / N][e % N] -= t0.a[e / N][e % N] + t1.a[e / N][e % N];
+#pragma unroll
+        for (int e = 0; e < N; ++e) rh.a[e] -= v0.a[e] + v1.a[e];
+        stv(row + 3 * NN, mv(inv(sch), rh));
+      }
+      __syncthreads();
+      const V<N> xl = ldv(blk + (nx1 - 1) * ROW + 3 * NN);
+      for (int r = tid; r < nr; r += nth) {
+        double *x = blk + r * ROW + 3 * NN;
+        const V<N> t = mv(ld(zb + r * NN), xl);
+#pragma unroll
+        for (int e = 0; e < N; ++e) x[e] -= t.a[e];
+      }
       __syncthreads();
     }
     // P7a: species correction (forward_backward.hpp:101-124) into dc
@@ -656,8 +743,10 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       for (int n = 1; n <= NY; ++n) dens += dv[n];
       dens = x[0] - dens;
       dv[0] = x[0];
+      if constexpr (!PER) {  // the periodic update leaves du_n as it is
 #pragma unroll
-      for (int n = 1; n <= NY; ++n) dv[n] += dens * wp[n * nc1 + i];
+        for (int n = 1; n <= NY; ++n) dv[n] += dens * wp[n * nc1 + i];
+      }
       dv[S::IVX] = x[1];
       if constexpr (N == 3) {
         dv[S::IPR] = x[2];
@@ -722,6 +811,55 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
   }
 }
 
+// launch shape of one x1 pencil launch: shared memory, grid, threads, and
+// whether the rows can travel by bulk copies
+struct ColLaunch {
+  Geom g;
+  size_t smem;
+  unsigned nblk;
+  int nthr;
+};
+
+inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double *w,
+                       const double *du, const double *u, const double *u1, ColLaunch &cl) {
+  const ColSmem L = col_smem(nv, g.nc1, g.nx1, nimpl, per ? 1 : 0);
+  cl.smem = sizeof(double) * (size_t)L.total;
+  if (cl.smem > 227 * 1024) {
+    set_error("x1 pencil too long for shared memory");
+    return CANOE_ERR_UNSUPPORTED;
+  }
+  cl.nblk = (unsigned)g.nx2 * (unsigned)g.nx3;
+  // threads per pencil: the kernel strides every loop by blockDim and needs
+  // at least two warps (warp 0 runs the scan while the others reconstruct)
+  cl.nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)
+                ? g.col_threads
+                : kColThreads;
+  // bulk copies move whole pencil rows: 16-byte aligned bases and an even
+  // row length keep every row 16-byte aligned
+  auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };
+  cl.g = g;
+  cl.g.bulk = (g.nc1 % 2 == 0) && al16(w) && al16(du) && al16(u) && al16(u1) ? 1 : 0;
+  return 0;
+}
+
+template <class K>
+int col_go(K kern, const ColLaunch &cl, const canoe_thermo_t &th, const double *w, double *du,
+           double *u, double *u1, const double *dtp, const Stage &s, int stage, double *fout,
+           cudaStream_t st) {
+  if (int rc = ensure_smem((const void *)kern, cl.smem)) return rc;
+  kern<<<cl.nblk, cl.nthr, cl.smem, st>>>(cl.g, th, w, du, u, u1, dtp, s, stage, fout);
+  CB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// implicit modes with periodic x1 at both ends; instantiated in
+// column_per_ny*.cu (column_per.cuh)
+template <int NY, typename R>
+int run_x1col_per(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int flag,
+                  int mode, const double *w, double *du, double *u, double *u1,
+                  const double *dtp, const Stage &s, int stage, double *fout,
+                  cudaStream_t st);
+
 // launcher for one NY (instantiated in column_ny*.cu)
 template <int NY, typename R>
 int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int flag,
@@ -730,28 +868,13 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
                 cudaStream_t st) {
   const int nimpl = (mode == kColFluxOnly || !(flag & 1)) ? 0 : ((flag & 8) ? 5 : 3);
   if (mode == kColSolveOnly && nimpl == 0) return 0;
-  const ColSmem L = col_smem(5 + NY, g.nc1, g.nx1, nimpl);
-  const size_t smem = sizeof(double) * (size_t)L.total;
-  if (smem > 227 * 1024) {
-    set_error("x1 pencil too long for shared memory");
-    return CANOE_ERR_UNSUPPORTED;
-  }
-  const unsigned nblk = (unsigned)g.nx2 * (unsigned)g.nx3;
-  // threads per pencil: the kernel strides every loop by blockDim and needs
-  // at least two warps (warp 0 runs the scan while the others reconstruct)
-  const int nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)
-                       ? g.col_threads
-                       : kColThreads;
-  // bulk copies move whole pencil rows: 16-byte aligned bases and an even
-  // row length keep every row 16-byte aligned
-  auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };
-  Geom gg = g;
-  gg.bulk = (g.nc1 % 2 == 0) && al16(w) && al16(du) && al16(u) && al16(u1) ? 1 : 0;
+  if (nimpl && g.bc[0] == CANOE_BC_PERIODIC)
+    return run_x1col_per<NY, R>(g, th, recon, rs, flag, mode, w, du, u, u1, dtp, s, stage,
+                                fout, st);
+  ColLaunch cl;
+  if (int rc = col_prepare(g, 5 + NY, nimpl, false, w, du, u, u1, cl)) return rc;
   auto go = [&](auto kern) -> int {
-    if (int rc = ensure_smem((const void *)kern, smem)) return rc;
-    kern<<<nblk, nthr, smem, st>>>(gg, th, w, du, u, u1, dtp, s, stage, fout);
-    CB_CUDA(cudaGetLastError());
-    return 0;
+    return col_go(kern, cl, th, w, du, u, u1, dtp, s, stage, fout, st);
   };
   const bool ppm = recon == CANOE_RECON_PPM, hllc = rs == CANOE_RSOLVER_HLLC;
   if (g.shell) {  // cubed-sphere panel: dry, FP64, HLLC

@@ -212,6 +212,46 @@ def moist3d(nx1=128, nx2=256, nx3=256, x1max=16.0e3, x2max=64.0e3, x3max=64.0e3,
     return Problem("C2-moist3d", cfg, x1f, u, w, dict(seed=seed))
 
 
+def periodic_x1(nx1=48, nx2=8, nx3=4, x1max=4800.0, x2max=800.0, x3max=400.0, moist=False,
+                v1=20.0, amp=0.02, seed=20240611, implicit_flag=1, recon=RECON_PPM,
+                rsolver=RS_HLLC, cfl=0.4):
+    """A box periodic in every direction and without gravity, for the cyclic
+    implicit x1 solve (periodic_forward_backward.hpp): uniform 300 K,
+    1e5 Pa air moving at v1 along x1, with a seeded density bump and seeded
+    velocity noise of relative size amp; moist=True adds H2O vapour at a
+    seeded mass fraction near 1e-3 and zero condensates (no saturation
+    adjustment)."""
+    th = T.earth_moist() if moist else T.dry()
+    th.grav = 0.0
+    ny = th.ny
+    nv = 5 + ny
+    x1f = np.linspace(0.0, x1max, nx1 + 1)
+    z = 0.5 * (x1f[1:] + x1f[:-1])
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shp = (nx3, nx2, nx1)
+    bump = 1.0 + amp * np.exp(-((z - 0.3 * x1max) / (0.1 * x1max)) ** 2)
+    w_int = np.zeros((nv,) + shp)
+    q = np.zeros((max(ny, 1),) + shp)
+    if ny:
+        q[0] = 1.0e-3 * (1.0 + 0.2 * rng.uniform(-1.0, 1.0, shp))
+    feps = T.feps_of(th, q[:ny]) if ny else 1.0
+    pres = 1.0e5 * (1.0 + 0.1 * amp * rng.uniform(-1.0, 1.0, shp))
+    w_int[0] = pres / (th.rd * feps * 300.0) * bump[None, None, :]
+    for n in range(1, ny + 1):
+        w_int[n] = q[n - 1]
+    w_int[1 + ny] = v1 * (1.0 + amp * rng.uniform(-1.0, 1.0, shp))
+    w_int[2 + ny] = v1 * amp * rng.uniform(-1.0, 1.0, shp)
+    w_int[3 + ny] = v1 * amp * rng.uniform(-1.0, 1.0, shp)
+    w_int[4 + ny] = pres
+    shape = _shape(nx1, nx2, nx3, nv)
+    u = _embed(shape, T.prim_to_cons(th, w_int), nx1, nx2, nx3)
+    w = _embed(shape, w_int, nx1, nx2, nx3)
+    bc = [BC_PERIODIC] * 6
+    cfg, x1f = make_config(nx1, nx2, nx3, x1f, x2max / nx2, x3max / nx3, th, bc, recon,
+                           rsolver, implicit_flag=implicit_flag, satadj=0, cfl=cfl)
+    return Problem("periodic-x1", cfg, x1f, u, w, dict(seed=seed))
+
+
 @dataclass
 class ShellProblem:
     """A cubed-sphere shell: config, radial faces, conserved and primitive

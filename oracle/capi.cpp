@@ -100,6 +100,11 @@ int oracle_block_solve_implicit(void *h, double *du, double dt) {
   return 0;
 }
 
+int oracle_periodic_block_solve(int nb, int n, const double *a, const double *b,
+                                const double *c, const double *rhs, double *x) {
+  return oracle::periodic_block_solve(nb, n, a, b, c, rhs, x);
+}
+
 int oracle_block_step(void *h, double dt, int nsteps) {
   Block &b = *static_cast<Block *>(h);
   try {

@@ -2,8 +2,10 @@
 // X1 direction: ImplicitSolver::SolveImplicit3D (src/snap/implicit/
 // solve_implicit_3d.cpp:91-142) -> PartialCorrection (partial_correction.cpp:
 // 26-170) / FullCorrection (full_correction.cpp:32-161) -> ForwardSweep /
-// BackwardSubstitution (forward_backward.hpp:15-137), single block per
-// column (first_block = last_block = true, no MPI pipeline), non-periodic x1.
+// BackwardSubstitution (forward_backward.hpp:15-137), or, with periodic x1,
+// PeriodicForwardSweep / PeriodicBackwardSubstitution
+// (periodic_forward_backward.hpp:15-234), single block per column
+// (first_block = last_block = true, no MPI pipeline).
 // Small dense matrices are plain arrays instead of Eigen; 3x3 inverses use
 // the adjugate, 5x5 inverses Gauss-Jordan with partial pivoting.
 // TEST INFRASTRUCTURE ONLY.
@@ -181,6 +183,77 @@ Mat<N> reduce(const Mat<5> &m) {
 }
 
 template <int N>
+Mat<N> sub(const Mat<N> &x, const Mat<N> &y) {
+  Mat<N> r;
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) r.a[i][j] = x.a[i][j] - y.a[i][j];
+  return r;
+}
+template <int N>
+Mat<N> neg(const Mat<N> &x) {
+  Mat<N> r;
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) r.a[i][j] = -x.a[i][j];
+  return r;
+}
+template <int N>
+Vec<N> sub(const Vec<N> &x, const Vec<N> &y) {
+  Vec<N> r;
+  for (int i = 0; i < N; ++i) r.a[i] = x.a[i] - y.a[i];
+  return r;
+}
+
+// El-Mikkawy (2005) cyclic block-tridiagonal solve of one column,
+// periodic_forward_backward.hpp:15-234 with first_block = last_block: the
+// row is couples to ie through the upper corner b[is] and the row ie to is
+// through the lower corner c[is-1] (the ghost row's upper block).  Leaves the
+// solution in delta.
+template <int N, class Rhs>
+void periodic_sweep(int is, int ie, const std::vector<Mat<N>> &a,
+                    const std::vector<Mat<N>> &bb, std::vector<Mat<N>> c, Rhs rhs_of,
+                    std::vector<Vec<N>> &delta) {
+  const size_t n = a.size();
+  std::vector<Mat<N>> ainv(n), gam(n), beta(n);
+  std::vector<Vec<N>> zeta(n);
+  Mat<N> sbg;
+  sbg.zero();
+  Vec<N> sbz;
+  for (int r = 0; r < N; ++r) sbz.a[r] = 0.;
+  // PeriodicForwardSweep (:61-172)
+  Vec<N> rhs = rhs_of(is);
+  ainv[is] = inverse(a[is]);
+  gam[is] = bb[is];
+  beta[is] = mul(c[is - 1], ainv[is]);
+  zeta[is] = rhs;
+  for (int i = is + 1; i <= ie; ++i) {
+    rhs = rhs_of(i);
+    const Mat<N> bl = mul(bb[i], ainv[i - 1]);
+    ainv[i] = inverse(sub(a[i], mul(bl, c[i - 1])));
+    gam[i] = mul(neg(bl), gam[i - 1]);
+    beta[i] = mul(mul(neg(beta[i - 1]), c[i - 1]), ainv[i]);
+    zeta[i] = sub(rhs, mul(bl, zeta[i - 1]));
+  }
+  gam[ie - 1] = sub(c[ie - 1], mul(mul(bb[ie - 1], ainv[ie - 2]), gam[ie - 2]));
+  beta[ie - 1] = mul(sub(bb[ie], mul(beta[ie - 2], c[ie - 2])), ainv[ie - 1]);
+  for (int i = is; i < ie; ++i) {
+    const Mat<N> t = mul(beta[i], gam[i]);
+    const Vec<N> v = mul(beta[i], zeta[i]);
+    for (int r = 0; r < N; ++r) {
+      sbz.a[r] += v.a[r];
+      for (int q = 0; q < N; ++q) sbg.a[r][q] += t.a[r][q];
+    }
+  }
+  ainv[ie] = inverse(sub(a[ie], sbg));
+  zeta[ie] = sub(rhs, sbz);
+  // PeriodicBackwardSubstitution (:176-204)
+  c[ie - 1].zero();
+  delta[ie] = mul(ainv[ie], zeta[ie]);
+  const Vec<N> last = delta[ie];
+  for (int i = ie - 1; i >= is; --i)
+    delta[i] = mul(ainv[i], sub(sub(zeta[i], mul(c[i], delta[i + 1])), mul(gam[i], last)));
+}
+
+template <int N>
 void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
   const int nc1 = b.nc1, nv = b.nv, ny = b.ny, IVX = b.ivx, IPR = b.ipr;
   const int is = b.is, ie = b.ie;
@@ -259,8 +332,9 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
       }
     Am = Ap;
   }
-  // reflecting ends (partial_correction.cpp:153-154)
-  {
+  const bool periodic = b.cfg.bc[0] == CANOE_BC_PERIODIC;
+  // reflecting ends (partial_correction.cpp:153-154); none when periodic
+  if (!periodic) {
     Mat<N> t = mul(bb[is], Bnd);
     for (int r = 0; r < N; ++r)
       for (int q = 0; q < N; ++q) a[is].a[r][q] += t.a[r][q];
@@ -284,6 +358,25 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
     }
     return r;
   };
+  if (periodic) {
+    periodic_sweep<N>(is, ie, a, bb, c, rhs_of, delta);
+    // the periodic update carries no species correction: du_n stays, and
+    // the dry density takes delta(0) minus the species
+    // (periodic_forward_backward.hpp:207-225)
+    for (int i = is; i <= ie; ++i) {
+      du[b.idx(0, k, j, i)] = delta[i].a[0];
+      du[b.idx(IVX, k, j, i)] = delta[i].a[1];
+      if constexpr (N == 3) {
+        du[b.idx(IPR, k, j, i)] = delta[i].a[2];
+      } else {
+        du[b.idx(IVX + 1, k, j, i)] = delta[i].a[2];
+        du[b.idx(IVX + 2, k, j, i)] = delta[i].a[3];
+        du[b.idx(IPR, k, j, i)] = delta[i].a[4];
+      }
+      for (int n = 1; n < IVX; ++n) du[b.idx(0, k, j, i)] -= du[b.idx(n, k, j, i)];
+    }
+    return;
+  }
   {
     Vec<N> rhs = rhs_of(is);
     a[is] = inverse(a[is]);
@@ -325,13 +418,43 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
   }
 }
 
+template <int N>
+void periodic_dense(int n, const double *a, const double *b, const double *c,
+                    const double *rhs, double *x) {
+  std::vector<Mat<N>> A(n + 1), B(n + 1), C(n + 1);
+  std::vector<Vec<N>> R(n + 1), D(n + 1);
+  for (int i = 0; i <= n; ++i)
+    for (int r = 0; r < N; ++r) {
+      R[i].a[r] = rhs[i * N + r];
+      for (int q = 0; q < N; ++q) {
+        A[i].a[r][q] = a[(i * N + r) * N + q];
+        B[i].a[r][q] = b[(i * N + r) * N + q];
+        C[i].a[r][q] = c[(i * N + r) * N + q];
+      }
+    }
+  periodic_sweep<N>(1, n, A, B, C, [&](int i) { return R[i]; }, D);
+  for (int i = 1; i <= n; ++i)
+    for (int r = 0; r < N; ++r) x[i * N + r] = D[i].a[r];
+}
+
 }  // namespace
+
+int periodic_block_solve(int nb, int n, const double *a, const double *b, const double *c,
+                         const double *rhs, double *x) {
+  if (n < 3) return 1;
+  if (nb == 3) periodic_dense<3>(n, a, b, c, rhs, x);
+  else if (nb == 5) periodic_dense<5>(n, a, b, c, rhs, x);
+  else return 1;
+  return 0;
+}
 
 void solve_implicit(Block &b, std::vector<double> &du, double dt) {
   int flag = b.cfg.implicit_flag;
   if (!(flag & 1)) return;
-  if (b.cfg.bc[0] == CANOE_BC_PERIODIC)
-    throw std::runtime_error("periodic x1 implicit solve is not supported");
+  if ((b.cfg.bc[0] == CANOE_BC_PERIODIC) != (b.cfg.bc[1] == CANOE_BC_PERIODIC))
+    throw std::runtime_error("x1 is periodic at one end only");
+  if (b.cfg.bc[0] == CANOE_BC_PERIODIC && b.ie - b.is + 1 < 3)
+    throw std::runtime_error("periodic x1 implicit solve needs at least 3 levels");
   bool full = flag & 8;
 #pragma omp parallel for collapse(2) schedule(dynamic, 16)
   for (int k = b.ks; k <= b.ke; ++k)

@@ -102,6 +102,11 @@ void calculate_fluxes_x1_only(Block &b);
 void add_flux_divergence(Block &b, double wght, std::vector<double> &du);
 void add_gravity_source(Block &b, double dt, std::vector<double> &du);
 void solve_implicit(Block &b, std::vector<double> &du, double dt);
+// the cyclic block-tridiagonal solve alone: rows 1..n of nb x nb blocks a, b,
+// c (row-major, n + 1 blocks each; c[0] is the lower corner, the coupling of
+// row n to row 1) and rhs; x receives rows 1..n
+int periodic_block_solve(int nb, int n, const double *a, const double *b, const double *c,
+                         const double *rhs, double *x);
 double new_dt(const Block &b);
 void step(Block &b, double dt);
 

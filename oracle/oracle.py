@@ -43,6 +43,8 @@ def load():
         ("oracle_block_calculate_fluxes", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         ("oracle_block_solve_implicit", c_int, [c_void_p, c_void_p, c_double]),
         ("oracle_block_step", c_int, [c_void_p, c_double, c_int]),
+        ("oracle_periodic_block_solve", c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p,
+                                                c_void_p, c_void_p]),
         ("oracle_block_new_dt", c_double, [c_void_p]),
         ("oracle_riemann", c_int, [c_int, POINTER(Thermo), c_int, c_void_p, c_void_p, c_void_p, c_int64]),
         ("oracle_cons_to_prim", c_int, [POINTER(Thermo), c_void_p, c_void_p, c_int64]),
@@ -137,6 +139,20 @@ class OracleBlock:
 
     def new_dt(self):
         return self.lib.oracle_block_new_dt(self.h)
+
+
+def periodic_block_solve(a, b, c, rhs):
+    """The oracle's El-Mikkawy cyclic block-tridiagonal solve.  a, b, c:
+    (n + 1, N, N) blocks of rows 0..n, of which rows 1..n are the system and
+    c[0] the lower corner (row n's coupling to row 1); rhs (n + 1, N).
+    Returns x (n + 1, N) with row 0 zero."""
+    a, b, c, rhs = (np.ascontiguousarray(v, dtype=np.float64) for v in (a, b, c, rhs))
+    n, nb = a.shape[0] - 1, a.shape[1]
+    x = np.zeros_like(rhs)
+    rc = load().oracle_periodic_block_solve(nb, n, _p(a), _p(b), _p(c), _p(rhs), _p(x))
+    if rc:
+        raise ValueError("periodic_block_solve: unsupported block size or n < 3")
+    return x
 
 
 def riemann(rsolver, th, ivx, wl, wr):
