@@ -70,13 +70,28 @@ int cuda_status(cudaError_t e, const char *what);
 // eos.cu).  `dtp` points at the device copy of the step's dt; every kernel
 // multiplies it by the stage's beta so that a step can be captured in a CUDA
 // graph without baking dt in.
-// x1 pencil kernel (column.cuh): mode 0 fluxes only (writes flx_out and the
-// x1 part of du), 1 full stage (fluxes + implicit solve + RK update of u),
-// 2 implicit solve of du only
+// x1 pencil kernel (column.cuh) modes.  kColFluxOnly: x1 fluxes out
+// (flx_out and the x1 part of du); kColStep: the fused stage (x1 divergence,
+// x1 solve, register update of u); kColSolveOnly: the x1 solve of a given du;
+// kColDivOnly: du += x1 divergence and sources, written back (the x2 / x3
+// solves run next); kColSolveStep: the x1 solve of the stored du and the
+// register update
+enum ColMode { kColFluxOnly = 0, kColStep = 1, kColSolveOnly = 2, kColDivOnly = 3,
+               kColSolveStep = 4 };
 int launch_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs,
                  int implicit_flag, int precision, int mode, const double *w, double *du, double *u,
                  double *u1, const double *dtp, const Stage &s, int stage,
                  double *flx_out, cudaStream_t st);
+// implicit solves along x2 (dir 1) and x3 (dir 2) of a dry block (lines.cu):
+// whether the flag asks for one in a direction the block has, the doubles
+// of each of the two line-major scratch arrays, and the solve of du in place
+// (wt, dut: scratch; dxl: nx_dir + 2 NGHOST line spacings)
+bool line_solve_on(const Geom &g, int implicit_flag, int dir);
+size_t line_scratch_doubles(const Geom &g, int implicit_flag);
+int launch_line_solve(int dir, const Geom &g, const canoe_thermo_t &th, int implicit_flag,
+                      const double *w, double *du, double *wt, double *dut,
+                      const double *dxl, const double *dtp, const Stage &s,
+                      cudaStream_t st);
 int launch_flux_x23(int dir, const Geom &g, const canoe_thermo_t &th, int recon,
                     int rs, int precision, const double *w, double *du,
                     const double *dtp, double beta, double *flx_out,

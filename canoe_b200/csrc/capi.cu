@@ -137,6 +137,10 @@ struct canoe_block {
   unsigned long long *d_dtacc = nullptr;
   unsigned long long *d_sat = nullptr;  // saturation-adjustment statistics
   uint32_t *d_err = nullptr;
+  // x2 / x3 implicit solves: line-major scratch of w and du, line spacings
+  // (nx2 + 2 NG entries of dx2, then nx3 + 2 NG of dx3)
+  double *d_wt = nullptr, *d_dut = nullptr, *d_dxl = nullptr;
+  bool lines = false;
   cudaStream_t st = nullptr;
   bool own_stream = false;
   cudaGraphExec_t gexec = nullptr;
@@ -152,7 +156,8 @@ static int block_free(canoe_block *b) {
   for (void *p : {(void *)b->d_u, (void *)b->d_w, (void *)b->d_u1, (void *)b->d_du,
                   (void *)b->d_x1f, (void *)b->d_x1v, (void *)b->d_dx1f,
                   (void *)b->d_scr, (void *)b->d_dt, (void *)b->d_pref, (void *)b->d_dtacc,
-                  (void *)b->d_err, (void *)b->d_sat})
+                  (void *)b->d_err, (void *)b->d_sat, (void *)b->d_wt, (void *)b->d_dut,
+                  (void *)b->d_dxl})
     if (p) cudaFree(p);
   if (b->own_stream && b->st) cudaStreamDestroy(b->st);
   delete b;
@@ -171,6 +176,19 @@ struct StepTimer {
     return 0;
   }
 };
+
+// the x3 then x2 implicit solves of du, in place (solve_implicit_3d.cpp:25-89)
+static int line_solves(canoe_block *b, double *du, const double *dtp, const Stage &sg) {
+  const Geom &g = b->g;
+  for (int dir = 2; dir >= 1; --dir) {
+    if (!line_solve_on(g, b->cfg.implicit_flag, dir)) continue;
+    const double *dxl = b->d_dxl + (dir == 2 ? g.nx2 + 2 * NG : 0);
+    if (int rc = launch_line_solve(dir, g, b->th, b->cfg.implicit_flag, b->d_w, du, b->d_wt,
+                                   b->d_dut, dxl, dtp, sg, b->st))
+      return rc;
+  }
+  return 0;
+}
 
 // one RK3 step, all launches on b->st; fixed_dt <= 0 uses the device dt
 static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullptr) {
@@ -196,10 +214,23 @@ static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullpt
                                       nullptr, b->st)))
       return rc;
     CB_MARK(2);
-    if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
-                           b->cfg.precision, kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt, sg, s,
-                           nullptr, b->st)))
-      return rc;
+    if (!b->lines) {
+      if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                             b->cfg.precision, kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt,
+                             sg, s, nullptr, b->st)))
+        return rc;
+    } else {
+      // du complete before the x3, x2, x1 solves (solve_implicit_3d.cpp:25-142)
+      if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                             b->cfg.precision, kColDivOnly, b->d_w, b->d_du, b->d_u, b->d_u1,
+                             b->d_dt, sg, s, nullptr, b->st)))
+        return rc;
+      if ((rc = line_solves(b, b->d_du, b->d_dt, sg))) return rc;
+      if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                             b->cfg.precision, kColSolveStep, b->d_w, b->d_du, b->d_u, b->d_u1,
+                             b->d_dt, sg, s, nullptr, b->st)))
+        return rc;
+    }
     CB_MARK(0);
     if (s == 2 && b->cfg.satadj && b->th.ny > 0) {
       canoe_satadj_opts_t o{1e-8, 30, b->mlp ? 2 : 0};
@@ -295,6 +326,14 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
     set_error("precision must be CANOE_FP64 or CANOE_FP32_PERTURBATION");
     return CANOE_ERR_ARG;
   }
+  if ((((cfg->implicit_flag & 2) && cfg->nx2 > 1) || ((cfg->implicit_flag & 4) && cfg->nx3 > 1)) &&
+      cfg->thermo.ny > 0) {
+    // the reference's moist x2 / x3 update reads w at the transposed
+    // indices (forward_backward.hpp:107-110 under solve_implicit_3d.cpp:
+    // 35-89), i.e. at unrelated cells
+    set_error("x2 / x3 implicit solves are provided for a dry block");
+    return CANOE_ERR_UNSUPPORTED;
+  }
   for (int i = 0; i < cfg->nx1; ++i)
     if (!(cfg->h_x1f[i + 1] > cfg->h_x1f[i])) {
       set_error("x1 faces must increase");
@@ -380,6 +419,19 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
   if ((e = cudaMemcpy(b->d_x1f, xf.data(), xf.size() * sizeof(double), cudaMemcpyHostToDevice))) return fail(e, "copy");
   if ((e = cudaMemcpy(b->d_x1v, xv.data(), xv.size() * sizeof(double), cudaMemcpyHostToDevice))) return fail(e, "copy");
   if ((e = cudaMemcpy(b->d_dx1f, dx.data(), dx.size() * sizeof(double), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  b->lines = line_solve_on(g, cfg->implicit_flag, 1) || line_solve_on(g, cfg->implicit_flag, 2);
+  if (b->lines) {
+    const size_t nl = line_scratch_doubles(g, cfg->implicit_flag) * sizeof(double);
+    if ((e = cudaMalloc(&b->d_wt, nl))) return fail(e, "cudaMalloc line scratch");
+    if ((e = cudaMalloc(&b->d_dut, nl))) return fail(e, "cudaMalloc line scratch");
+    const int n2 = g.nx2 + 2 * NG, n3 = g.nx3 + 2 * NG;
+    std::vector<double> dl(n2 + n3);
+    for (int q = 0; q < n2; ++q) dl[q] = g.dx2;
+    for (int q = 0; q < n3; ++q) dl[n2 + q] = g.dx3;
+    if ((e = cudaMalloc(&b->d_dxl, dl.size() * sizeof(double)))) return fail(e, "cudaMalloc dxl");
+    if ((e = cudaMemcpy(b->d_dxl, dl.data(), dl.size() * sizeof(double), cudaMemcpyHostToDevice)))
+      return fail(e, "copy");
+  }
   if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking))) return fail(e, "stream");
   b->own_stream = true;
   g.x1f = b->d_x1f;
@@ -480,10 +532,12 @@ int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt) {
     set_error("null du or non-positive dt");
     return CANOE_ERR_ARG;
   }
-  if (!(b->cfg.implicit_flag & 1)) return 0;
+  if (!(b->cfg.implicit_flag & 1) && !b->lines) return 0;
   // the solve reads dt through the device dt slot: use slot 1 as a scratch
   CB_CUDA(cudaMemcpyAsync(b->d_dt + 1, &dt, sizeof(double), cudaMemcpyHostToDevice, b->st));
   const Stage one{0., 1., 1.};
+  if (b->lines)
+    if (int rc = line_solves(b, d_du, b->d_dt + 1, one)) return rc;
   int rc = launch_x1col(b->g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
                         b->cfg.precision, kColSolveOnly, b->d_w, d_du, b->d_u, b->d_u1, b->d_dt + 1, one, 1,
                         nullptr, b->st);

@@ -33,7 +33,6 @@
 
 namespace cb {
 
-enum ColMode { kColFluxOnly = 0, kColStep = 1, kColSolveOnly = 2 };
 
 // threads per pencil: 5 warps cover the nx1 + 1 faces and nx1 + 2 cells of a
 // 128-level column in one pass
@@ -127,8 +126,10 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
   const double grav = th.grav;
   const double wght = st.beta * dtp[0];
   const bool bulk = g.bulk != 0;
-  constexpr bool NEED_DU = MODE == kColSolveOnly || MODE == kColStep;
-  const bool load_du = NEED_DU && (MODE == kColSolveOnly || g.f2);
+  constexpr bool SOLVE_ONLY = MODE == kColSolveOnly || MODE == kColSolveStep;
+  constexpr bool UPDATE = MODE == kColStep || MODE == kColSolveStep;
+  constexpr bool NEED_DU = MODE != kColFluxOnly;
+  const bool load_du = NEED_DU && (SOLVE_ONLY || g.f2);
   const uint32_t row_bytes = (uint32_t)nc1 * 8u;
 
   // a wait that gave up: report, give the copies still in flight on
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
   }
 
   constexpr bool PERT = sizeof(R) == 4;
-  if constexpr (MODE != kColSolveOnly) {
+  if constexpr (!SOLVE_ONLY) {
     R *q = reinterpret_cast<R *>(un);          // [NV][nc1] transformed copy, later F
     R *WL = q + NV * nc1;                      // [NV][nc1]
     R *WR = WL + NV * nc1;                     // [NV][nc1]
@@ -571,7 +572,7 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     __syncthreads();
     // u and u1 travel into the |A| / J area while the reduction runs
     double *su = sA, *su1 = sA + NV * nc1;
-    const bool pre_u = bulk && MODE == kColStep;
+    const bool pre_u = bulk && UPDATE;
     if (pre_u && tid == 0) {
       mbar_expect_tx(mbar + 2, (stage == 0 ? 1 : 2) * NV * row_bytes);
       for (int n = 0; n < NV; ++n) bulk_g2s(su + n * nc1, u + n * g.sv + base, row_bytes, mbar + 2);
@@ -768,7 +769,7 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
     } else {
       __syncthreads();
     }
-    if constexpr (MODE == kColStep) {
+    if constexpr (UPDATE) {
       if (pre_u) {
         for (int n = 0; n < NV; ++n)
           for (int i = is + tid; i <= ie; i += nth) {
@@ -790,7 +791,7 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
   }
 
   // P7b: write back
-  if constexpr (MODE == kColSolveOnly) {
+  if constexpr (!UPDATE) {
     for (int n = 0; n < NV; ++n)
       for (int i = is + tid; i <= ie; i += nth) du[n * g.sv + base + i] = dc[n * nc1 + i];
   } else {
@@ -866,7 +867,8 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
                 int mode, const double *w, double *du, double *u, double *u1,
                 const double *dtp, const Stage &s, int stage, double *fout,
                 cudaStream_t st) {
-  const int nimpl = (mode == kColFluxOnly || !(flag & 1)) ? 0 : ((flag & 8) ? 5 : 3);
+  const int nimpl =
+      (mode == kColFluxOnly || mode == kColDivOnly || !(flag & 1)) ? 0 : ((flag & 8) ? 5 : 3);
   if (mode == kColSolveOnly && nimpl == 0) return 0;
   if (nimpl && g.bc[0] == CANOE_BC_PERIODIC)
     return run_x1col_per<NY, R>(g, th, recon, rs, flag, mode, w, du, u, u1, dtp, s, stage,
@@ -886,8 +888,8 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
 #define CB_GCOL(NIMPL, MODE) \
   (ppm ? go(k_x1col<NY, 3, 1, NIMPL, MODE, R, 1>) : go(k_x1col<NY, 2, 1, NIMPL, MODE, R, 1>))
       if (mode == kColFluxOnly) return CB_GCOL(0, kColFluxOnly);
-      if (mode == kColSolveOnly) {
-        set_error("solve-only mode is not provided on a cubed-sphere panel");
+      if (mode != kColStep) {
+        set_error("only the fused stage is provided on a cubed-sphere panel");
         return CANOE_ERR_UNSUPPORTED;
       }
       if (nimpl == 0) return CB_GCOL(0, kColStep);
@@ -903,9 +905,14 @@ int run_x1col_p(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int 
   (ppm ? (hllc ? go(k_x1col<NY, 3, 1, NIMPL, MODE, R>) : go(k_x1col<NY, 3, 0, NIMPL, MODE, R>)) \
        : (hllc ? go(k_x1col<NY, 2, 1, NIMPL, MODE, R>) : go(k_x1col<NY, 2, 0, NIMPL, MODE, R>)))
   if (mode == kColFluxOnly) return CB_COL(0, kColFluxOnly);
+  if (mode == kColDivOnly) return CB_COL(0, kColDivOnly);
   if (mode == kColSolveOnly)
     return nimpl == 3 ? go(k_x1col<NY, 3, 1, 3, kColSolveOnly, double>)
                       : go(k_x1col<NY, 3, 1, 5, kColSolveOnly, double>);
+  if (mode == kColSolveStep)
+    return nimpl == 0   ? go(k_x1col<NY, 3, 1, 0, kColSolveStep, double>)
+           : nimpl == 3 ? go(k_x1col<NY, 3, 1, 3, kColSolveStep, double>)
+                        : go(k_x1col<NY, 3, 1, 5, kColSolveStep, double>);
   if (nimpl == 0) return CB_COL(0, kColStep);
   if (nimpl == 3) return CB_COL(3, kColStep);
   return CB_COL(5, kColStep);
@@ -917,7 +924,7 @@ int run_x1col(const Geom &g, const canoe_thermo_t &th, int recon, int rs, int fl
               int prec, int mode, const double *w, double *du, double *u, double *u1,
               const double *dtp, const Stage &s, int stage, double *fout,
               cudaStream_t st) {
-  if (prec == CANOE_FP32_PERTURBATION && mode != kColSolveOnly)
+  if (prec == CANOE_FP32_PERTURBATION && mode != kColSolveOnly && mode != kColSolveStep)
     return run_x1col_p<NY, float>(g, th, recon, rs, flag, mode, w, du, u, u1, dtp, s, stage,
                                   fout, st);
   return run_x1col_p<NY, double>(g, th, recon, rs, flag, mode, w, du, u, u1, dtp, s, stage,

@@ -25,6 +25,9 @@ int run_x1col_per(const Geom &g, const canoe_thermo_t &th, int recon, int rs, in
   if (mode == kColSolveOnly)
     return nimpl == 3 ? go(k_x1col<NY, 3, 1, 3, kColSolveOnly, double, 0, true>)
                       : go(k_x1col<NY, 3, 1, 5, kColSolveOnly, double, 0, true>);
+  if (mode == kColSolveStep)
+    return nimpl == 3 ? go(k_x1col<NY, 3, 1, 3, kColSolveStep, double, 0, true>)
+                      : go(k_x1col<NY, 3, 1, 5, kColSolveStep, double, 0, true>);
   const bool ppm = recon == CANOE_RECON_PPM, hllc = rs == CANOE_RSOLVER_HLLC;
 #define CB_PCOL(NIMPL)                                                                    \
   (ppm ? (hllc ? go(k_x1col<NY, 3, 1, NIMPL, kColStep, R, 0, true>)                        \

@@ -88,8 +88,13 @@ __global__ void __launch_bounds__(256)
         else
           d1 /= (fabs(wc[S::IVX]) + cs);
         dtc = d1;
-        if (g.f2) dtc = fmin(dtc, g.dx2 / (fabs(wc[S::IVY]) + cs));
-        if (g.f3) dtc = fmin(dtc, g.dx3 / (fabs(wc[S::IVZ]) + cs));
+        // implicit x2 / x3: |v| only, as in x1
+        if (g.f2)
+          dtc = fmin(dtc, (imp & 2) ? g.dx2 / (cfl * fabs(wc[S::IVY]))
+                                    : g.dx2 / (fabs(wc[S::IVY]) + cs));
+        if (g.f3)
+          dtc = fmin(dtc, (imp & 4) ? g.dx3 / (cfl * fabs(wc[S::IVZ]))
+                                    : g.dx3 / (fabs(wc[S::IVZ]) + cs));
       }
     }
   }

@@ -795,6 +795,10 @@ int canoe_shell_create(const canoe_shell_config_t *cfg, canoe_shell_t *out) {
     set_error("canoe_shell_create: periodic radial boundaries are not supported");
     return CANOE_ERR_UNSUPPORTED;
   }
+  if (cfg->implicit_flag & 6) {
+    set_error("canoe_shell_create: the shell's implicit solve is radial (implicit_flag 1 or 9)");
+    return CANOE_ERR_UNSUPPORTED;
+  }
   canoe_shell *s = new canoe_shell();
   s->cfg = *cfg;
   s->cfg.h_x1f = nullptr;

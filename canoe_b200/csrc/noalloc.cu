@@ -115,6 +115,11 @@ extern "C" int canoe_block_step_noalloc(const canoe_block_config_t *cfg, double 
   g.sv = (int64_t)g.nc3 * g.sk;
   g.dx2 = cfg->dx2;
   g.dx3 = cfg->dx3;
+  if (line_solve_on(g, cfg->implicit_flag, 1) || line_solve_on(g, cfg->implicit_flag, 2)) {
+    set_error("canoe_block_step_noalloc: x2 / x3 implicit solves need line scratch; use "
+              "canoe_block_step");
+    return CANOE_ERR_UNSUPPORTED;
+  }
   const size_t nvals = (size_t)g.nv * (size_t)g.sv;
   const size_t need = 2 * nvals + 4 * (size_t)g.nc1 + 8;
   if (need > kNoAllocDoubles) {

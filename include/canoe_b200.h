@@ -112,7 +112,9 @@ typedef struct canoe_block_config {
   const double *h_x1f;    /* nx1+1 interior x1 face positions (nonuniform ok) */
   int32_t recon;          /* canoe_recon                                      */
   int32_t rsolver;        /* canoe_rsolver                                    */
-  int32_t implicit_flag;  /* bit0 X1, bit3 full 5x5 (implicit_solver.cpp:47)  */
+  int32_t implicit_flag;  /* bit0 X1, bit1 X2, bit2 X3, bit3 full 5x5
+                           * (implicit_solver.cpp:47, solve_implicit_3d.cpp:
+                           * 25-142); X2 / X3 on dry blocks only          */
   int32_t precision;      /* canoe_precision                                  */
   int32_t satadj;         /* 1: saturation adjustment at the last RK stage    */
   double cfl;             /* CFL number for canoe_block_new_dt                */
@@ -245,12 +247,16 @@ int canoe_block_set_stream(canoe_block_t b, void *stream);
 int canoe_block_calculate_fluxes(canoe_block_t b, double *d_flx1,
                                  double *d_flx2, double *d_flx3);
 
-/* ImplicitSolver::SolveImplicit3D(du, w, dt), X1 direction:
- * canoe src/snap/implicit/solve_implicit_3d.cpp:91-142 with
- * PartialCorrection (partial_correction.cpp:26-170) or FullCorrection
- * (full_correction.cpp:32-161) and ForwardSweep / BackwardSubstitution
- * (forward_backward.hpp:15-137).  d_du (NV, nc3, nc2, nc1) is corrected in
- * place; the block's current primitive state is used as w. */
+/* ImplicitSolver::SolveImplicit3D(du, w, dt): canoe src/snap/implicit/
+ * solve_implicit_3d.cpp:19-142, the directions of implicit_flag in the
+ * reference's order X3, X2, X1, each with PartialCorrection
+ * (partial_correction.cpp:26-170) or FullCorrection (full_correction.cpp:
+ * 32-161) and ForwardSweep / BackwardSubstitution (forward_backward.hpp:
+ * 15-137), or the periodic sweep (periodic_forward_backward.hpp:15-234) when
+ * both ends of the direction are periodic.  X2 / X3 write back IDN, the
+ * normal momentum and IEN, as the reference's transposition does.  d_du
+ * (NV, nc3, nc2, nc1) is corrected in place; the block's current primitive
+ * state is used as w. */
 int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt);
 
 /* One full time step of the block (all RK3 stages): the Athena task list as
@@ -283,7 +289,9 @@ int canoe_block_step(canoe_block_t b, double dt);
  * any stream capture begins.  All calls on a device share the array, so
  * calls that overlap in time (other streams or threads) race and corrupt
  * each other's results: order them on one stream.  The saturation
- * adjustment (cfg->satadj) uses the cold start. */
+ * adjustment (cfg->satadj) uses the cold start.  X2 / X3 implicit solves
+ * (implicit_flag bits 1, 2) need line scratch: such a cfg returns
+ * CANOE_ERR_UNSUPPORTED. */
 int canoe_block_step_noalloc(const canoe_block_config_t *cfg, double *d_u, double *d_w,
                              uint32_t *d_err, double dt, void *stream);
 

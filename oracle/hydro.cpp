@@ -690,7 +690,8 @@ void add_gravity_source(Block &b, double dt, std::vector<double> &du) {
 }
 
 // Hydro::NewBlockTimeStep with canoe patches/21.new_blockdt.patch:20-40
-// (implicit X1 uses |v1| only); returns cfl * min over interior cells.
+// (an implicit direction uses |v| only: x1 when nx2 > 1, x2 and x3 by their
+// bits); returns cfl * min over interior cells.
 double new_dt(const Block &b) {
   double cfl = b.cfg.cfl;
   bool imp1 = (b.cfg.implicit_flag & 1) && (b.nx2 > 1);
@@ -707,8 +708,13 @@ double new_dt(const Block &b) {
         if (imp1) dt1 /= cfl * std::fabs(wi[b.ivx]);
         else dt1 /= (std::fabs(wi[b.ivx]) + cs);
         mn = std::min(mn, dt1);
-        if (b.f2) mn = std::min(mn, b.dx2 / (std::fabs(wi[b.ivy]) + cs));
-        if (b.f3) mn = std::min(mn, b.dx3 / (std::fabs(wi[b.ivz]) + cs));
+        const int flag = b.cfg.implicit_flag;
+        if (b.f2)
+          mn = std::min(mn, (flag & 2) ? b.dx2 / (cfl * std::fabs(wi[b.ivy]))
+                                       : b.dx2 / (std::fabs(wi[b.ivy]) + cs));
+        if (b.f3)
+          mn = std::min(mn, (flag & 4) ? b.dx3 / (cfl * std::fabs(wi[b.ivz]))
+                                       : b.dx3 / (std::fabs(wi[b.ivz]) + cs));
       }
   return cfl * mn;
 }
@@ -738,7 +744,7 @@ void step(Block &b, double dt) {
     double wght = be[stage] * dt;
     add_flux_divergence(b, wght, b.du);
     add_gravity_source(b, wght, b.du);
-    if (b.cfg.implicit_flag & 1) solve_implicit(b, b.du, wght);
+    if (b.cfg.implicit_flag & 7) solve_implicit(b, b.du, wght);
 #pragma omp parallel for collapse(3) schedule(static)
     for (int n = 0; n < b.nv; ++n)
       for (int k = b.ks; k <= b.ke; ++k)

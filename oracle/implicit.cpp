@@ -253,11 +253,28 @@ void periodic_sweep(int is, int ie, const std::vector<Mat<N>> &a,
     delta[i] = mul(ainv[i], sub(sub(zeta[i], mul(c[i], delta[i + 1])), mul(gam[i], last)));
 }
 
+// One implicit line of direction dir (0: x1, 1: x2, 2: x3) through the cell
+// (k, j, i) with the line index replaced: PartialCorrection / FullCorrection
+// with mydir_ = dir.  The line's primitives are read with the velocity in the
+// direction's frame (normal, then the next two cyclically), as CopyPrimitives,
+// FluxJacobian and Eigenvector do (flux_decomposition.hpp:14-120); the
+// reference transposes du (solve_implicit_3d.cpp:35-56, 68-89) and writes back
+// IDN, the normal momentum and IEN only.
 template <int N>
-void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
+void column(Block &b, std::vector<double> &du, double dt, int dir, int k, int j, int i0) {
   const int nc1 = b.nc1, nv = b.nv, ny = b.ny, IVX = b.ivx, IPR = b.ipr;
-  const int is = b.is, ie = b.ie;
+  const int lo = dir == 0 ? b.is : dir == 1 ? b.js : b.ks;
+  const int hi = dir == 0 ? b.ie : dir == 1 ? b.je : b.ke;
+  const int is = lo, ie = hi;
+  const int nline = (dir == 0 ? b.nc1 : dir == 1 ? b.nc2 : b.nc3);
   const size_t s = b.cells();
+  // flat offset of line position t
+  auto at = [&](int t) -> size_t {
+    if (dir == 0) return b.idx(0, k, j, t);
+    if (dir == 1) return b.idx(0, k, t, i0);
+    return b.idx(0, t, j, i0);
+  };
+  const int vn = IVX + dir, vt1 = IVX + (1 + dir) % 3, vt2 = IVX + (2 + dir) % 3;
   // a cubed-sphere panel projects the velocities onto the local frame
   // for the solve (solve_implicit_3d.cpp:105-117)
   double cos_t = 0., sin_t = 1.;
@@ -265,17 +282,24 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
     cos_t = b.geo->cosc[b.geo->kj(k, j)];
     sin_t = b.geo->sinc[b.geo->kj(k, j)];
   }
-  auto W = [&](int i, double *out) {
-    for (int n = 0; n < nv; ++n) out[n] = b.w[b.idx(0, k, j, i) + n * s];
+  auto W = [&](int t, double *out) {
+    const size_t c = at(t);
+    for (int n = 0; n < nv; ++n) out[n] = b.w[c + n * s];
+    if (dir != 0) {
+      const double a = out[vn], bb = out[vt1], cc = out[vt2];
+      out[IVX] = a;
+      out[IVX + 1] = bb;
+      out[IVX + 2] = cc;
+    }
     if (b.geo) {
       out[IVX + 1] += out[IVX + 2] * cos_t;
       out[IVX + 2] *= sin_t;
     }
   };
   const double gm1 = b.th.gammad - 1.;
-  const double grav = b.th.grav;
-  std::vector<Mat<N>> a(nc1), bb(nc1), c(nc1), dfdq(nc1);
-  std::vector<Vec<N>> delta(nc1);
+  const double grav = dir == 0 ? b.th.grav : 0.;  // Phi acts in x1 only
+  std::vector<Mat<N>> a(nline), bb(nline), c(nline), dfdq(nline);
+  std::vector<Vec<N>> delta(nline);
   Mat<5> full;
   double wl[CANOE_MAX_NV], wr[CANOE_MAX_NV], prim[CANOE_MAX_NV];
   // flux Jacobians of cells is-2..ie+1 (partial_correction.cpp:90-101)
@@ -309,6 +333,8 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
   Mat<N> Am = reduce<N>(full), Ap;
   const double area = b.dx2 * b.dx3;
   for (int i = is - 1; i <= ie; ++i) {
+    // face areas and the cell volume (GetFace{1,2,3}Area, GetCellVolume of
+    // the Cartesian block; partial_correction.cpp:116-127)
     W(i, wl);
     W(i + 1, wr);
     roe_average(prim, gm1, wl, wr, ny);
@@ -316,6 +342,13 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
     abs_jacobian(full, prim, cs, gm1, ny);
     Ap = reduce<N>(full);
     double aleft = area, aright = area, vol = b.dx1f[i] * b.dx2 * b.dx3;
+    if (dir == 1) {
+      aleft = aright = b.dx1f[i0] * b.dx3;
+      vol = b.dx1f[i0] * b.dx2 * b.dx3;
+    } else if (dir == 2) {
+      aleft = aright = b.dx1f[i0] * b.dx2;
+      vol = b.dx1f[i0] * b.dx2 * b.dx3;
+    }
     if (b.geo) {  // GetFace1Area / GetCellVolume of the panel
       aleft = shell_face1_area(b, k, j, i);
       aright = shell_face1_area(b, k, j, i + 1);
@@ -332,7 +365,7 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
       }
     Am = Ap;
   }
-  const bool periodic = b.cfg.bc[0] == CANOE_BC_PERIODIC;
+  const bool periodic = b.cfg.bc[2 * dir] == CANOE_BC_PERIODIC;
   // reflecting ends (partial_correction.cpp:153-154); none when periodic
   if (!periodic) {
     Mat<N> t = mul(bb[is], Bnd);
@@ -343,37 +376,49 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
       for (int q = 0; q < N; ++q) a[ie].a[r][q] += t.a[r][q];
   }
   // ForwardSweep (forward_backward.hpp:15-85)
+  auto D = [&](int n, int t) -> double & { return du[at(t) + n * s]; };
   auto rhs_of = [&](int i) {
     Vec<N> r;
-    double r0 = du[b.idx(0, k, j, i)];
-    for (int n = 1; n < IVX; ++n) r0 += du[b.idx(n, k, j, i)];
+    double r0 = D(0, i);
+    for (int n = 1; n < IVX; ++n) r0 += D(n, i);
     r.a[0] = r0 / dt;
-    r.a[1] = du[b.idx(IVX, k, j, i)] / dt;
+    r.a[1] = D(vn, i) / dt;
     if constexpr (N == 3) {
-      r.a[2] = du[b.idx(IPR, k, j, i)] / dt;
+      r.a[2] = D(IPR, i) / dt;
     } else {
-      r.a[2] = du[b.idx(IVX + 1, k, j, i)] / dt;
-      r.a[3] = du[b.idx(IVX + 2, k, j, i)] / dt;
-      r.a[4] = du[b.idx(IPR, k, j, i)] / dt;
+      r.a[2] = D(vt1, i) / dt;
+      r.a[3] = D(vt2, i) / dt;
+      r.a[4] = D(IPR, i) / dt;
     }
     return r;
   };
+  // x2 / x3: the reference copies back IDN, the normal momentum and IEN
+  // (solve_implicit_3d.cpp:46-55, 79-88); the other slots of du stay
+  auto put_line = [&](int i, const Vec<N> &x) {
+    D(0, i) = x.a[0];
+    D(vn, i) = x.a[1];
+    D(IPR, i) = x.a[N - 1];
+  };
   if (periodic) {
     periodic_sweep<N>(is, ie, a, bb, c, rhs_of, delta);
+    if (dir != 0) {  // dry only (checked by the caller)
+      for (int i = is; i <= ie; ++i) put_line(i, delta[i]);
+      return;
+    }
     // the periodic update carries no species correction: du_n stays, and
     // the dry density takes delta(0) minus the species
     // (periodic_forward_backward.hpp:207-225)
     for (int i = is; i <= ie; ++i) {
-      du[b.idx(0, k, j, i)] = delta[i].a[0];
-      du[b.idx(IVX, k, j, i)] = delta[i].a[1];
+      D(0, i) = delta[i].a[0];
+      D(IVX, i) = delta[i].a[1];
       if constexpr (N == 3) {
-        du[b.idx(IPR, k, j, i)] = delta[i].a[2];
+        D(IPR, i) = delta[i].a[2];
       } else {
-        du[b.idx(IVX + 1, k, j, i)] = delta[i].a[2];
-        du[b.idx(IVX + 2, k, j, i)] = delta[i].a[3];
-        du[b.idx(IPR, k, j, i)] = delta[i].a[4];
+        D(IVX + 1, i) = delta[i].a[2];
+        D(IVX + 2, i) = delta[i].a[3];
+        D(IPR, i) = delta[i].a[4];
       }
-      for (int n = 1; n < IVX; ++n) du[b.idx(0, k, j, i)] -= du[b.idx(n, k, j, i)];
+      for (int n = 1; n < IVX; ++n) D(0, i) -= D(n, i);
     }
     return;
   }
@@ -399,22 +444,25 @@ void column(Block &b, std::vector<double> &du, double dt, int k, int j) {
     Vec<N> t = mul(a[i], delta[i + 1]);
     for (int r = 0; r < N; ++r) delta[i].a[r] -= t.a[r];
   }
+  if (dir != 0) {  // dry only (checked by the caller)
+    for (int i = is; i <= ie; ++i) put_line(i, delta[i]);
+    return;
+  }
   for (int i = is; i <= ie; ++i) {
-    double dens = du[b.idx(0, k, j, i)];
-    for (int n = 1; n < IVX; ++n) dens += du[b.idx(n, k, j, i)];
+    double dens = D(0, i);
+    for (int n = 1; n < IVX; ++n) dens += D(n, i);
     dens = delta[i].a[0] - dens;
-    du[b.idx(0, k, j, i)] = delta[i].a[0];
-    for (int n = 1; n < IVX; ++n)
-      du[b.idx(n, k, j, i)] += dens * b.w[b.idx(n, k, j, i)];
-    du[b.idx(IVX, k, j, i)] = delta[i].a[1];
+    D(0, i) = delta[i].a[0];
+    for (int n = 1; n < IVX; ++n) D(n, i) += dens * b.w[b.idx(n, k, j, i)];
+    D(IVX, i) = delta[i].a[1];
     if constexpr (N == 3) {
-      du[b.idx(IPR, k, j, i)] = delta[i].a[2];
+      D(IPR, i) = delta[i].a[2];
     } else {
-      du[b.idx(IVX + 1, k, j, i)] = delta[i].a[2];
-      du[b.idx(IVX + 2, k, j, i)] = delta[i].a[3];
-      du[b.idx(IPR, k, j, i)] = delta[i].a[4];
+      D(IVX + 1, i) = delta[i].a[2];
+      D(IVX + 2, i) = delta[i].a[3];
+      D(IPR, i) = delta[i].a[4];
     }
-    for (int n = 1; n < IVX; ++n) du[b.idx(0, k, j, i)] -= du[b.idx(n, k, j, i)];
+    for (int n = 1; n < IVX; ++n) D(0, i) -= D(n, i);
   }
 }
 
@@ -449,21 +497,41 @@ int periodic_block_solve(int nb, int n, const double *a, const double *b, const 
 }
 
 void solve_implicit(Block &b, std::vector<double> &du, double dt) {
-  int flag = b.cfg.implicit_flag;
-  if (!(flag & 1)) return;
-  if ((b.cfg.bc[0] == CANOE_BC_PERIODIC) != (b.cfg.bc[1] == CANOE_BC_PERIODIC))
-    throw std::runtime_error("x1 is periodic at one end only");
-  if (b.cfg.bc[0] == CANOE_BC_PERIODIC && b.ie - b.is + 1 < 3)
-    throw std::runtime_error("periodic x1 implicit solve needs at least 3 levels");
-  bool full = flag & 8;
+  const int flag = b.cfg.implicit_flag;
+  const bool full = flag & 8;
+  const bool x3 = (flag & 4) && b.cfg.nx3 > 1, x2 = (flag & 2) && b.cfg.nx2 > 1;
+  if ((x2 || x3) && (b.ny > 0 || b.geo))
+    throw std::runtime_error("x2 / x3 implicit solves are provided for a dry Cartesian block");
+  for (int d = 0; d < 3; ++d) {
+    const bool p0 = b.cfg.bc[2 * d] == CANOE_BC_PERIODIC, p1 = b.cfg.bc[2 * d + 1] == CANOE_BC_PERIODIC;
+    const bool on = d == 0 ? (flag & 1) : d == 1 ? x2 : x3;
+    if (!on) continue;
+    if (p0 != p1) throw std::runtime_error("a periodic direction needs both boundaries periodic");
+    const int n = d == 0 ? b.cfg.nx1 : d == 1 ? b.cfg.nx2 : b.cfg.nx3;
+    if (p0 && n < 3) throw std::runtime_error("a periodic implicit solve needs at least 3 cells");
+  }
+  auto run = [&](int d, int k, int j, int i) {
+    if (full)
+      column<5>(b, du, dt, d, k, j, i);
+    else
+      column<3>(b, du, dt, d, k, j, i);
+  };
+  // solve_implicit_3d.cpp:25-142: X3, then X2, then X1
+  if (x3) {
 #pragma omp parallel for collapse(2) schedule(dynamic, 16)
-  for (int k = b.ks; k <= b.ke; ++k)
-    for (int j = b.js; j <= b.je; ++j) {
-      if (full)
-        column<5>(b, du, dt, k, j);
-      else
-        column<3>(b, du, dt, k, j);
-    }
+    for (int j = b.js; j <= b.je; ++j)
+      for (int i = b.is; i <= b.ie; ++i) run(2, 0, j, i);
+  }
+  if (x2) {
+#pragma omp parallel for collapse(2) schedule(dynamic, 16)
+    for (int k = b.ks; k <= b.ke; ++k)
+      for (int i = b.is; i <= b.ie; ++i) run(1, k, 0, i);
+  }
+  if (flag & 1) {
+#pragma omp parallel for collapse(2) schedule(dynamic, 16)
+    for (int k = b.ks; k <= b.ke; ++k)
+      for (int j = b.js; j <= b.je; ++j) run(0, k, j, 0);
+  }
 }
 
 }  // namespace oracle
