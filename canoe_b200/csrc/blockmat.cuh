@@ -124,6 +124,62 @@ __device__ __forceinline__ M<5> inv(const M<5> &m) {
   return r;
 }
 
+// Row-parallel 5x5 algebra for the cyclic reduction of the full system.  An
+// 8-lane segment of a warp holds one 5x5 block: lane g < 5 owns row g, lanes
+// 5..7 follow along (their results are never stored).  Shuffles stay inside
+// the segment (width 8, mask smask of the segment's lanes).
+
+// Gauss-Jordan inverse with partial pivoting of the block whose row g is
+// ar[], the steps of inv(M<5>) with the pivot rows left in place: at column c
+// the largest |ar[c]| among the lanes not yet used as pivots (lowest lane on
+// a tie) normalises its row and eliminates column c from every other row.
+// On return iv[] is row `pivot_of` of the inverse, where pivot_of is the
+// column this lane was the pivot for (rows 0..4 are held by lanes 0..4 in
+// some order).
+__device__ __forceinline__ int inv5_rows(double ar[5], double iv[5], int g,
+                                         unsigned smask) {
+#pragma unroll
+  for (int q = 0; q < 5; ++q) iv[q] = (q == g) ? 1. : 0.;
+  int mine = -1;  // the column this lane pivoted
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    double v = (g < 5 && mine < 0) ? fabs(ar[c]) : -1.;
+    int p = g;
+#pragma unroll
+    for (int off = 4; off >= 1; off >>= 1) {
+      const double ov = __shfl_xor_sync(smask, v, off, 8);
+      const int op = __shfl_xor_sync(smask, p, off, 8);
+      if (ov > v || (ov == v && op < p)) {
+        v = ov;
+        p = op;
+      }
+    }
+    const double ip = 1. / __shfl_sync(smask, ar[c], p, 8);
+    if (g == p) {
+      mine = c;
+#pragma unroll
+      for (int q = c + 1; q < 5; ++q) ar[q] *= ip;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) iv[q] *= ip;
+    }
+    double pr[5], pi[5];
+#pragma unroll
+    for (int q = c + 1; q < 5; ++q) pr[q] = __shfl_sync(smask, ar[q], p, 8);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) pi[q] = __shfl_sync(smask, iv[q], p, 8);
+    if (g != p) {
+      const double f = ar[c];
+      if (f != 0.) {
+#pragma unroll
+        for (int q = c + 1; q < 5; ++q) ar[q] -= f * pr[q];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) iv[q] -= f * pi[q];
+      }
+    }
+  }
+  return mine;
+}
+
 // row / column selection of the reduced (partial) system: (rho, m1, E)
 template <int N>
 __device__ __forceinline__ constexpr int sel(int r) {

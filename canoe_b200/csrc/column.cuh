@@ -37,6 +37,15 @@ namespace cb {
 // threads per pencil: 5 warps cover the nx1 + 1 faces and nx1 + 2 cells of a
 // 128-level column in one pass
 constexpr int kColThreads = 160;
+// the full 5x5 solve runs row-parallel (8-lane segments per block row-op)
+// and takes 10 warps per pencil
+constexpr int kCol5Threads = 320;
+
+template <int N, bool PER>
+struct ColBounds {
+  static constexpr int threads = (N == 5 && !PER) ? kCol5Threads : kColThreads;
+  static constexpr int blocks = N == 5 ? 1 : 3;
+};
 
 template <int N>
 struct ColRow {
@@ -100,7 +109,7 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
 // reference's periodic du update without the species correction
 // (periodic_forward_backward.hpp:207-225).
 template <int NY, int RECON, int RS, int N, int MODE, typename R, int GEO = 0, bool PER = false>
-__global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
+__global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>::blocks)
     k_x1col(Geom g, canoe_thermo_t th, const double *__restrict__ w,
             double *__restrict__ du, double *__restrict__ u, double *__restrict__ u1,
             const double *__restrict__ dtp, Stage st, int stage,
@@ -552,7 +561,10 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
           row[2 * NN + e] = i == ie ? 0. : c;
         }
       }
-      stm(row, ((r & 1) == 0 && 1 < nr && r < nr) ? inv(am) : am);
+      if constexpr (N == 5 && !PER)
+        stm(row, am);  // the row-parallel reduction inverts its pivots itself
+      else
+        stm(row, ((r & 1) == 0 && 1 < nr && r < nr) ? inv(am) : am);
       // right-hand side (forward_backward.hpp:24-41)
       double r0 = dc[i];
 #pragma unroll
@@ -670,41 +682,198 @@ __global__ void __launch_bounds__(kColThreads, N == 5 ? 1 : 3)
       stv(row + 3 * NN, mv(ai, rh));
       if constexpr (PER) stm(zb + r * NN, mm(ai, zr));
     };
-    int stop = 1;  // first s with 2 s - 1 >= nr
-    while (2 * stop - 1 < nr) stop *= 2;
-    int s = 1;
-    for (; s < stop && nr / (2 * s) > 32; s *= 2) {
-      for (int m = tid; m < nr / (2 * s); m += nth) level(s, m);
+    if constexpr (N == 5 && !PER) {
+      // row-parallel reduction: an 8-lane segment per block row-op, lane
+      // g < 5 owning row g of the 5x5 blocks (blockmat.cuh inv5_rows); the
+      // neighbours' blocks are read as shared-memory broadcasts
+      const int seg = tid >> 3, nseg = nth >> 3, g = tid & 7, gg = g < 5 ? g : 0;
+      const unsigned smask = 0xFFu << (tid & 24);
+      // the block of row r: its a replaced by a^-1 in place
+      auto invert_row = [&](int r) {
+        double *row = blk + r * ROW;
+        double ar[5], iv[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) ar[q] = row[gg * 5 + q];
+        const int c = inv5_rows(ar, iv, g, smask);
+        if (g < 5 && c >= 0)
+#pragma unroll
+          for (int q = 0; q < 5; ++q) row[c * 5 + q] = iv[q];
+      };
+      auto level5 = [&](int s, int m) {
+        const int r = 2 * s * (m + 1) - 1;
+        double *row = blk + r * ROW;
+        const double *lo = blk + (r - s) * ROW;
+        double ar[5], br[5], cr[5], al[5], bn[5], cn[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          ar[q] = row[gg * 5 + q];
+          br[q] = row[NN + gg * 5 + q];
+          cr[q] = row[2 * NN + gg * 5 + q];
+        }
+        double rh = row[3 * NN + gg];
+        // alpha = -b a_lo^-1
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          double t = 0.;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) t += br[k] * lo[k * 5 + q];
+          al[q] = -t;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          double t = 0., u = 0.;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) {
+            t += al[k] * lo[2 * NN + k * 5 + q];
+            u += al[k] * lo[NN + k * 5 + q];
+          }
+          ar[q] += t;
+          bn[q] = u;
+        }
+        {
+          double t = 0.;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) t += al[k] * lo[3 * NN + k];
+          rh += t;
+        }
+        if (r + s < nr) {
+          const double *hi = blk + (r + s) * ROW;
+          double ga[5];
+#pragma unroll
+          for (int q = 0; q < 5; ++q) {
+            double t = 0.;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) t += cr[k] * hi[k * 5 + q];
+            ga[q] = -t;
+          }
+#pragma unroll
+          for (int q = 0; q < 5; ++q) {
+            double t = 0., u = 0.;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+              t += ga[k] * hi[NN + k * 5 + q];
+              u += ga[k] * hi[2 * NN + k * 5 + q];
+            }
+            ar[q] += t;
+            cn[q] = u;
+          }
+          double t = 0.;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) t += ga[k] * hi[3 * NN + k];
+          rh += t;
+        } else {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) cn[q] = 0.;
+        }
+        // every lane has read row r before any writes it (the shuffles of
+        // the inverse and the data dependence order them)
+        const bool next_elim = (m & 1) == 0 && 4 * s - 1 < nr;
+        if (next_elim) {
+          double iv[5];
+          const int c = inv5_rows(ar, iv, g, smask);
+          if (g < 5 && c >= 0)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) row[c * 5 + q] = iv[q];
+        } else if (g < 5) {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) row[g * 5 + q] = ar[q];
+        }
+        if (g < 5) {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) {
+            row[NN + g * 5 + q] = bn[q];
+            row[2 * NN + g * 5 + q] = cn[q];
+          }
+          row[3 * NN + g] = rh;
+        }
+      };
+      auto back5 = [&](int s, int m) {
+        const int r = s - 1 + 2 * s * m;
+        double *row = blk + r * ROW;
+        double t = row[3 * NN + gg];
+        if (r - s >= 0) {
+          const double *x = blk + (r - s) * ROW + 3 * NN;
+          double u = 0.;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) u += row[NN + gg * 5 + k] * x[k];
+          t -= u;
+        }
+        if (r + s < nr) {
+          const double *x = blk + (r + s) * ROW + 3 * NN;
+          double u = 0.;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) u += row[2 * NN + gg * 5 + k] * x[k];
+          t -= u;
+        }
+        double xr = 0.;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) xr += row[gg * 5 + k] * __shfl_sync(smask, t, k, 8);
+        if (g < 5) row[3 * NN + g] = xr;
+      };
+      int stop = 1;  // first s with 2 s - 1 >= nr
+      while (2 * stop - 1 < nr) stop *= 2;
+      if (1 < nr)
+        for (int m = seg; 2 * m < nr; m += nseg) invert_row(2 * m);
       __syncthreads();
-    }
-    const int s_warp = s;  // first level done by warp 0
-    // first back level done by all threads: the largest s with > 32 rows
-    int sb = 1;
-    while (2 * sb < stop && (nr + 2 * sb) / (4 * sb) > 32) sb *= 2;
-    if ((nr + sb) / (2 * sb) <= 32) sb = 0;  // every back level fits in warp 0
-    if (warp == 0) {
-      for (s = s_warp; s < stop; s *= 2) {
-        for (int m = lane; m < nr / (2 * s); m += 32) level(s, m);
-        __syncwarp();
+      for (int s = 1; s < stop; s *= 2) {
+        for (int m = seg; m < nr / (2 * s); m += nseg) level5(s, m);
+        __syncthreads();
       }
       // the last surviving row r = stop - 1 is decoupled
-      if (lane == 0) {
+      if (seg == 0) {
         double *row = blk + (stop - 1) * ROW;
-        M<N> ai = inv(ld(row));
-        stm(row, ai);
-        stv(row + 3 * NN, mv(ai, ldv(row + 3 * NN)));
-        if constexpr (PER) stm(zb + (stop - 1) * NN, mm(ai, ld(zb + (stop - 1) * NN)));
+        double ar[5], iv[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) ar[q] = row[gg * 5 + q];
+        const double rr = row[3 * NN + gg];
+        const int c = inv5_rows(ar, iv, g, smask);
+        double x = 0.;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) x += iv[k] * __shfl_sync(smask, rr, k, 8);
+        if (g < 5 && c >= 0) row[3 * NN + c] = x;
       }
-      __syncwarp();
-      for (s = stop / 2; s >= 1 && s > sb; s /= 2) {
-        for (int m = lane; m < (nr + s) / (2 * s); m += 32) back(s, m);
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    for (s = sb; s >= 1; s /= 2) {
-      for (int m = tid; m < (nr + s) / (2 * s); m += nth) back(s, m);
       __syncthreads();
+      for (int s = stop / 2; s >= 1; s /= 2) {
+        for (int m = seg; m < (nr + s) / (2 * s); m += nseg) back5(s, m);
+        __syncthreads();
+      }
+    } else {
+      int stop = 1;  // first s with 2 s - 1 >= nr
+      while (2 * stop - 1 < nr) stop *= 2;
+      int s = 1;
+      for (; s < stop && nr / (2 * s) > 32; s *= 2) {
+        for (int m = tid; m < nr / (2 * s); m += nth) level(s, m);
+        __syncthreads();
+      }
+      const int s_warp = s;  // first level done by warp 0
+      // first back level done by all threads: the largest s with > 32 rows
+      int sb = 1;
+      while (2 * sb < stop && (nr + 2 * sb) / (4 * sb) > 32) sb *= 2;
+      if ((nr + sb) / (2 * sb) <= 32) sb = 0;  // every back level fits in warp 0
+      if (warp == 0) {
+        for (s = s_warp; s < stop; s *= 2) {
+          for (int m = lane; m < nr / (2 * s); m += 32) level(s, m);
+          __syncwarp();
+        }
+        // the last surviving row r = stop - 1 is decoupled
+        if (lane == 0) {
+          double *row = blk + (stop - 1) * ROW;
+          M<N> ai = inv(ld(row));
+          stm(row, ai);
+          stv(row + 3 * NN, mv(ai, ldv(row + 3 * NN)));
+          if constexpr (PER) stm(zb + (stop - 1) * NN, mm(ai, ld(zb + (stop - 1) * NN)));
+        }
+        __syncwarp();
+        for (s = stop / 2; s >= 1 && s > sb; s /= 2) {
+          for (int m = lane; m < (nr + s) / (2 * s); m += 32) back(s, m);
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      for (s = sb; s >= 1; s /= 2) {
+        for (int m = tid; m < (nr + s) / (2 * s); m += nth) back(s, m);
+        __syncthreads();
+      }
     }
     if constexpr (PER) {
       // rows 0..n-2 hold y and Z with x = y - Z x(n-1); row n-1:
@@ -835,6 +1004,7 @@ inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double 
   cl.nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)
                 ? g.col_threads
                 : kColThreads;
+  if (nimpl == 5 && !per) cl.nthr = kCol5Threads;
   // bulk copies move whole pencil rows: 16-byte aligned bases and an even
   // row length keep every row 16-byte aligned
   auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };

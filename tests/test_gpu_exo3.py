@@ -76,7 +76,7 @@ def test_fluxes_match_oracle(oracle_mod):
         assert rel_l2(g1[:, n, jk, jk, NG:NG + nx1 + 1], r1[:, n, jk, jk, NG:NG + nx1 + 1]) < 2e-11, ("x1", n)
 
 
-@pytest.mark.parametrize("implicit_flag", [0, 1])
+@pytest.mark.parametrize("implicit_flag", [0, 1, 9])
 def test_step_matches_oracle(oracle_mod, implicit_flag):
     p = problems.shell_c3(nx1=16, nside=8, implicit_flag=implicit_flag)
     ora = oracle_mod.OracleShell(p)
