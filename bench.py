@@ -147,7 +147,8 @@ def make_problem(args, nx2=None, nx3=None):
     from canoe_b200 import problems
     return problems.moist3d(nx1=args.nx1, nx2=nx2 or args.nx2, nx3=nx3 or args.nx3,
                             x1max=16.0e3, x2max=64.0e3 * (nx2 or args.nx2) / 256,
-                            x3max=64.0e3 * (nx3 or args.nx3) / 256)
+                            x3max=64.0e3 * (nx3 or args.nx3) / 256,
+                            implicit_flag=getattr(args, "implicit_flag", 1))
 
 
 def algorithmic_bytes(nv, ny, ncell):
@@ -290,6 +291,57 @@ def c3_report(steps=10, warmup=3, nx1=64, nside=96, dt=60.0):
     return out
 
 
+def full5x5_report(args, net, steps=5, warmup=2):
+    """C2 with the full 5x5 implicit correction (implicit_flag 9, the
+    FullCorrection of most of the reference's example inputs): mixed +
+    learned against plain FP64, whole steps and the x1 pencil per launch."""
+    import torch
+    from canoe_b200 import MeshBlock
+    from canoe_b200._abi import FP32_PERTURBATION, FP64, check, load
+    lib = load()
+    p = make_problem(args)
+    p.cfg.implicit_flag = 9
+    ncell = p.cfg.nx1 * p.cfg.nx2 * p.cfg.nx3
+    stream = torch.cuda.Stream()
+    out = {"config": f"{p.cfg.nx1}x{p.cfg.nx2}x{p.cfg.nx3}, PPM + HLLC, implicit x1 full 5x5",
+           "unit": UNIT}
+    states, dt0 = {}, None
+    for name, prec in (("mixed", FP32_PERTURBATION), ("fp64", FP64)):
+        p.cfg.precision = prec
+        blk = MeshBlock(p, graph=True)
+        check(lib.canoe_block_set_stream(blk.h, ctypes.c_void_p(stream.cuda_stream)))
+        if name == "mixed":
+            blk.set_mlp(net)
+        dt0 = dt0 or blk.new_dt()
+        blk.set_fixed_dt(dt0)
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                blk.step()
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                blk.step()
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            prof = (ctypes.c_float * 7)()
+            check(lib.canoe_block_step_profile(blk.h, -1.0, prof, 7))
+            stream.synchronize()
+        rec = {"ms_per_step": ms / steps, "value": ncell * steps / (ms * 1e-3),
+               "x1_pencil_ms_per_launch": prof[0] / 3, "error_word": blk.error_word()}
+        states[name] = p.interior(blk.conserved())
+        out[name] = rec
+        blk.close()
+    a, b = states["mixed"], states["fp64"]
+    out["l2_error_mixed_vs_fp64"] = {
+        "state": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+        "steps": warmup + steps + 1}
+    out["value"] = out["mixed"]["value"]
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def c5_report(net, steps=5, warmup=2):
     """C5: 48 uneven blocks of C2 physics stepped as one CUDA graph with
     autotuned threads per x1 pencil, mixed + learned and plain FP64, against
@@ -369,7 +421,9 @@ def run_reference(args, rank):
 
 def config_dict(args):
     return {"workload": f"C2 3-D moist convection LES {args.nx1}x{args.nx2}x{args.nx3}, "
-                        "PPM + HLLC, implicit X1 partial 3x3, saturation adjustment each step",
+                        "PPM + HLLC, implicit X1 "
+                        + ("partial 3x3" if args.implicit_flag == 1 else "full 5x5")
+                        + ", saturation adjustment each step",
             "cells": args.nx1 * args.nx2 * args.nx3, "nv": 8, "rk_stages": 3,
             "precision": {"fp64": "FP64", "mixed": "FP32 fluxes on the hydrostatic "
                           "perturbation, FP64 implicit / accumulation / saturation "
@@ -395,6 +449,10 @@ def main():
     ap.add_argument("--no-c4", action="store_true")
     ap.add_argument("--no-c3", action="store_true")
     ap.add_argument("--no-c5", action="store_true")
+    ap.add_argument("--implicit-flag", type=int, default=1, choices=[1, 9],
+                    help="C2's implicit solve: 1 partial 3x3 (the headline), 9 full 5x5")
+    ap.add_argument("--no-5x5", action="store_true",
+                    help="skip the full 5x5 implicit variant of C2")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
                     help="c2: the headline line; c3 / c5: only that report, as one JSON line")
     args = ap.parse_args()
@@ -575,6 +633,9 @@ def main():
     c5 = None
     if rank == 0 and not args.no_c5:
         c5 = c5_report(net)
+    f5 = None
+    if rank == 0 and not args.no_5x5:
+        f5 = full5x5_report(args, net)
     if rank == 0 and not args.no_c4:
         c4 = c4_report(net, p.cfg.thermo)
     if dist:
@@ -594,6 +655,7 @@ def main():
             "c4_learned_warm_start": c4,
             "c3_cubed_sphere_shell": c3,
             "c5_batched_blocks": c5,
+            "c2_full5x5": f5,
             "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
             "error_word": err}
     print(json.dumps(line), flush=True)

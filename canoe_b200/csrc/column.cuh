@@ -37,14 +37,14 @@ namespace cb {
 // threads per pencil: 5 warps cover the nx1 + 1 faces and nx1 + 2 cells of a
 // 128-level column in one pass
 constexpr int kColThreads = 160;
-// the full 5x5 solve runs row-parallel (8-lane segments per block row-op)
-// and takes 10 warps per pencil
-constexpr int kCol5Threads = 320;
+// the full 5x5 solve runs row-parallel (8-lane segments per block row-op),
+// 7 warps per pencil and two pencils per SM
+constexpr int kCol5Threads = 224;
 
 template <int N, bool PER>
 struct ColBounds {
   static constexpr int threads = (N == 5 && !PER) ? kCol5Threads : kColThreads;
-  static constexpr int blocks = N == 5 ? 1 : 3;
+  static constexpr int blocks = N == 5 ? (PER ? 1 : 2) : 3;
 };
 
 template <int N>
@@ -71,7 +71,14 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
   int solve = 0;
   s.stg = 0;
   s.z = 0;
-  if (n_impl) {
+  if (n_impl == 5 && !per) {
+    // compact plan of the row-parallel 5x5 solve: |A| and J are staged in
+    // the rows' own c and b slots (plus three blocks past the last row, at
+    // stg), and u / u1 are not prefetched
+    const int rows = even_up(nx1 * ((3 * 25 + 5) | 1));
+    s.stg = s.uni + rows;
+    solve = rows + 3 * 25;
+  } else if (n_impl) {
     const int nn = n_impl * n_impl;
     const int rows = even_up(nx1 * ((3 * nn + n_impl) | 1));
     // |A| and J, later reused as the staging area of u and u1
@@ -452,6 +459,18 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
     double *blk = un;                        // [nx1][ROW]
     double *sA = sm + L.stg;                 // [nx1+1][NN] |A| at faces is-1/2..ie+1/2
     double *sJ = sA + (nx1 + 1) * NN;        // [nx1+2][NN] J of cells is-1..ie+1
+    // COMPACT (row-parallel 5x5): |A| at face t < nx1 sits in row t's c
+    // slot, J of cell is-1+t < nx1 in row t's b slot, the last three blocks
+    // at stg
+    constexpr bool COMPACT = N == 5 && !PER;
+    auto pA = [&](int t) -> double * {
+      if constexpr (COMPACT) return t < nx1 ? blk + t * ROW + 2 * NN : sA;
+      else return sA + t * NN;
+    };
+    auto pJ = [&](int t) -> double * {
+      if constexpr (COMPACT) return t < nx1 ? blk + t * ROW + NN : sA + (t - nx1 + 1) * NN;
+      else return sJ + t * NN;
+    };
     const double gm1 = th.gammad - 1.;
     const double dt = wght;
     const double idt = 1. / dt;
@@ -475,7 +494,7 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
       M<N> J;
       jacobian<N, NY>(J, gm1, wl);
 #pragma unroll
-      for (int e = 0; e < NN; ++e) sJ[t * NN + e] = J.a[e / N][e % N];
+      for (int e = 0; e < NN; ++e) pJ(t)[e] = J.a[e / N][e % N];
       if (t <= nx1) {
 #pragma unroll
         for (int n = 0; n < NV; ++n) wr[n] = wp[n * nc1 + ic + 1];
@@ -486,7 +505,7 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
         M<N> A;
         abs_jacobian<N, NY>(A, th, gm1, wl, wr);
 #pragma unroll
-        for (int e = 0; e < NN; ++e) sA[t * NN + e] = A.a[e / N][e % N];
+        for (int e = 0; e < NN; ++e) pA(t)[e] = A.a[e / N][e % N];
       }
     }
     __syncthreads();
@@ -520,16 +539,94 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
     // c of the ghost row is-1 (periodic_forward_backward.hpp:67-72).
     const int nr = PER ? nx1 - 1 : nx1;
     double *zb = sm + L.z;  // PER: [nr][NN]
-    for (int r = tid; r < nx1; r += nth) {
+    // face areas and the cell volume's reciprocal doubled, of row r
+    auto row_geom = [&](int r, double &aL, double &aR, double &i2v) {
       const int i = is + r;
-      double aL = area, aR = area;
-      double i2v = 1. / (2. * (g.dx1f[i] * g.dx2 * g.dx3));
+      aL = area;
+      aR = area;
+      i2v = 1. / (2. * (g.dx1f[i] * g.dx2 * g.dx3));
       if constexpr (GEO) {  // GetFace1Area / GetCellVolume
         const double d2 = tab(kTabDx2A, k, j), d3 = tab(kTabDx3A, k, j), sc = tab(kTabSinC, k, j);
         aL = d2 * d3 * g.x1f[i] * g.x1f[i] * sc;
         aR = d2 * d3 * g.x1f[i + 1] * g.x1f[i + 1] * sc;
         i2v = 1. / (2. * (g.dx1f[i] * d2 * d3 * g.x1v[i] * g.x1v[i] * sc));
       }
+    };
+    auto put_rhs = [&](int r) {  // forward_backward.hpp:24-41
+      const int i = is + r;
+      double r0 = dc[i];
+#pragma unroll
+      for (int n = 1; n <= NY; ++n) r0 += dc[n * nc1 + i];
+      double *rh = blk + r * ROW + 3 * NN;
+      rh[0] = r0 / dt;
+      rh[1] = dc[S::IVX * nc1 + i] / dt;
+      if constexpr (N == 3) {
+        rh[2] = dc[S::IPR * nc1 + i] / dt;
+      } else {
+        rh[2] = dc[S::IVY * nc1 + i] / dt;
+        rh[3] = dc[S::IVZ * nc1 + i] / dt;
+        rh[4] = dc[S::IPR * nc1 + i] / dt;
+      }
+    };
+    if constexpr (COMPACT) {
+      // a and the right-hand side first; b and c overwrite the staged J and
+      // |A| one matrix row at a time, after every row has read them
+      for (int r = tid; r < nx1; r += nth) {
+        const int i = is + r;
+        double aL, aR, i2v;
+        row_geom(r, aL, aR, i2v);
+        const double *Am = pA(r), *Ap = pA(r + 1), *Jm = pJ(r), *Jc = pJ(r + 1), *Jn = pJ(r + 2);
+        double *row = blk + r * ROW;
+#pragma unroll
+        for (int e = 0; e < NN; ++e) {
+          const int rr = e / N, qq = e % N;
+          const double phi = ((rr == 1 && qq == 0) || (rr == 4 && qq == 1)) ? grav : 0.;
+          double a = (Am[e] * aL + Ap[e] * aR + (aR - aL) * Jc[e]) * i2v + (rr == qq ? idt : 0.) - phi;
+          if (i == is) {
+            const double b = -(Am[e] + Jm[e]) * aL * i2v;
+            a += (qq == 1 ? -b : b);
+          }
+          if (i == ie) {
+            const double c = -(Ap[e] - Jn[e]) * aR * i2v;
+            a += (qq == 1 ? -c : c);
+          }
+          row[e] = a;
+        }
+        put_rhs(r);
+      }
+      for (int r0 = 0; r0 < nx1; r0 += nth) {
+        const int r = r0 + tid, i = is + r;
+        const bool on = r < nx1;
+        double aL = 0., aR = 0., i2v = 0.;
+        if (on) row_geom(r, aL, aR, i2v);
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+          double bv[N], cv[N];
+          if (on) {
+            const double *Am = pA(r) + q * N, *Ap = pA(r + 1) + q * N;
+            const double *Jm = pJ(r) + q * N, *Jn = pJ(r + 2) + q * N;
+#pragma unroll
+            for (int kk = 0; kk < N; ++kk) {
+              bv[kk] = i == is ? 0. : -(Am[kk] + Jm[kk]) * aL * i2v;
+              cv[kk] = i == ie ? 0. : -(Ap[kk] - Jn[kk]) * aR * i2v;
+            }
+          }
+          __syncthreads();
+          if (on) {
+            double *row = blk + r * ROW;
+#pragma unroll
+            for (int kk = 0; kk < N; ++kk) {
+              row[NN + q * N + kk] = bv[kk];
+              row[2 * NN + q * N + kk] = cv[kk];
+            }
+          }
+        }
+      }
+    }
+    if constexpr (!COMPACT) for (int r = tid; r < nx1; r += nth) {
+      const int i = is + r;
+      double aL, aR, i2v;
+      row_geom(r, aL, aR, i2v);
       double *row = blk + r * ROW;
       M<N> am;
 #pragma unroll
@@ -561,30 +658,14 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
           row[2 * NN + e] = i == ie ? 0. : c;
         }
       }
-      if constexpr (N == 5 && !PER)
-        stm(row, am);  // the row-parallel reduction inverts its pivots itself
-      else
-        stm(row, ((r & 1) == 0 && 1 < nr && r < nr) ? inv(am) : am);
-      // right-hand side (forward_backward.hpp:24-41)
-      double r0 = dc[i];
-#pragma unroll
-      for (int n = 1; n <= NY; ++n) r0 += dc[n * nc1 + i];
-      double *rh = row + 3 * NN;
-      rh[0] = r0 / dt;
-      rh[1] = dc[S::IVX * nc1 + i] / dt;
-      if constexpr (N == 3) {
-        rh[2] = dc[S::IPR * nc1 + i] / dt;
-      } else {
-        rh[2] = dc[S::IVY * nc1 + i] / dt;
-        rh[3] = dc[S::IVZ * nc1 + i] / dt;
-        rh[4] = dc[S::IPR * nc1 + i] / dt;
-      }
+      stm(row, ((r & 1) == 0 && 1 < nr && r < nr) ? inv(am) : am);
+      put_rhs(r);
     }
     if (bulk) fence_proxy_async();
     __syncthreads();
     // u and u1 travel into the |A| / J area while the reduction runs
     double *su = sA, *su1 = sA + NV * nc1;
-    const bool pre_u = bulk && UPDATE;
+    const bool pre_u = bulk && UPDATE && !COMPACT;
     if (pre_u && tid == 0) {
       mbar_expect_tx(mbar + 2, (stage == 0 ? 1 : 2) * NV * row_bytes);
       for (int n = 0; n < NV; ++n) bulk_g2s(su + n * nc1, u + n * g.sv + base, row_bytes, mbar + 2);
