@@ -40,11 +40,18 @@ constexpr int kColThreads = 160;
 // the full 5x5 solve runs row-parallel (8-lane segments per block row-op),
 // 7 warps per pencil and two pencils per SM
 constexpr int kCol5Threads = 224;
+// the 3x3 solve with the compact plan: 4 warps per pencil, four per SM
+constexpr bool kCompact3 = true;
+constexpr int kCol3Threads = 128;
 
-template <int N, bool PER>
-struct ColBounds {
-  static constexpr int threads = (N == 5 && !PER) ? kCol5Threads : kColThreads;
-  static constexpr int blocks = N == 5 ? (PER ? 1 : 2) : 3;
+// the compact shared-memory plan (|A| and J staged in the rows' own slots,
+// no u / u1 prefetch): the 5x5 solve, and the 3x3 one when kCompact3
+template <int N, bool PER, int GEO>
+struct ColPlan {
+  static constexpr bool compact = !PER && (N == 5 || (N == 3 && kCompact3 && !GEO));
+  static constexpr int threads =
+      !compact ? kColThreads : (N == 5 ? kCol5Threads : kCol3Threads);
+  static constexpr int blocks = N == 5 ? (PER ? 1 : 2) : (compact ? 4 : 3);
 };
 
 template <int N>
@@ -62,7 +69,8 @@ struct ColSmem {
 
 __host__ __device__ inline int even_up(int x) { return (x + 1) & ~1; }
 
-__host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl, int per = 0) {
+__host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl, int per = 0,
+                                            int compact = 0) {
   ColSmem s;
   s.wp = 0;                  // [NV][nc1] pristine pencil
   s.dc = nv * nc1;           // [NV][nc1] du of the column (interior at is)
@@ -71,13 +79,14 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
   int solve = 0;
   s.stg = 0;
   s.z = 0;
-  if (n_impl == 5 && !per) {
-    // compact plan of the row-parallel 5x5 solve: |A| and J are staged in
-    // the rows' own c and b slots (plus three blocks past the last row, at
-    // stg), and u / u1 are not prefetched
-    const int rows = even_up(nx1 * ((3 * 25 + 5) | 1));
+  if (n_impl && compact) {
+    // compact plan: |A| and J are staged in the rows' own c and b slots
+    // (plus three blocks past the last row, at stg), and u / u1 are not
+    // prefetched
+    const int nn = n_impl * n_impl;
+    const int rows = even_up(nx1 * ((3 * nn + n_impl) | 1));
     s.stg = s.uni + rows;
-    solve = rows + 3 * 25;
+    solve = rows + 3 * nn;
   } else if (n_impl) {
     const int nn = n_impl * n_impl;
     const int rows = even_up(nx1 * ((3 * nn + n_impl) | 1));
@@ -116,7 +125,7 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
 // reference's periodic du update without the species correction
 // (periodic_forward_backward.hpp:207-225).
 template <int NY, int RECON, int RS, int N, int MODE, typename R, int GEO = 0, bool PER = false>
-__global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>::blocks)
+__global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER, GEO>::blocks)
     k_x1col(Geom g, canoe_thermo_t th, const double *__restrict__ w,
             double *__restrict__ du, double *__restrict__ u, double *__restrict__ u1,
             const double *__restrict__ dtp, Stage st, int stage,
@@ -125,7 +134,7 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
   constexpr int NV = S::NV;
   extern __shared__ double sm[];
   const int nc1 = g.nc1, is = g.is, ie = g.ie, nx1 = g.nx1;
-  const ColSmem L = col_smem(NV, nc1, nx1, N, PER);
+  const ColSmem L = col_smem(NV, nc1, nx1, N, PER, ColPlan<N, PER, GEO>::compact);
   double *wp = sm + L.wp;
   double *dc = sm + L.dc;
   double *un = sm + L.uni;
@@ -462,7 +471,7 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
     // COMPACT (row-parallel 5x5): |A| at face t < nx1 sits in row t's c
     // slot, J of cell is-1+t < nx1 in row t's b slot, the last three blocks
     // at stg
-    constexpr bool COMPACT = N == 5 && !PER;
+    constexpr bool COMPACT = ColPlan<N, PER, GEO>::compact;
     auto pA = [&](int t) -> double * {
       if constexpr (COMPACT) return t < nx1 ? blk + t * ROW + 2 * NN : sA;
       else return sA + t * NN;
@@ -577,10 +586,11 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
         row_geom(r, aL, aR, i2v);
         const double *Am = pA(r), *Ap = pA(r + 1), *Jm = pJ(r), *Jc = pJ(r + 1), *Jn = pJ(r + 2);
         double *row = blk + r * ROW;
+        M<N> am;
 #pragma unroll
         for (int e = 0; e < NN; ++e) {
           const int rr = e / N, qq = e % N;
-          const double phi = ((rr == 1 && qq == 0) || (rr == 4 && qq == 1)) ? grav : 0.;
+          const double phi = ((rr == 1 && qq == 0) || (rr == N - 1 && qq == 1)) ? grav : 0.;
           double a = (Am[e] * aL + Ap[e] * aR + (aR - aL) * Jc[e]) * i2v + (rr == qq ? idt : 0.) - phi;
           if (i == is) {
             const double b = -(Am[e] + Jm[e]) * aL * i2v;
@@ -590,8 +600,13 @@ __global__ void __launch_bounds__(ColBounds<N, PER>::threads, ColBounds<N, PER>:
             const double c = -(Ap[e] - Jn[e]) * aR * i2v;
             a += (qq == 1 ? -c : c);
           }
-          row[e] = a;
+          if constexpr (N == 5)
+            row[e] = a;  // the row-parallel reduction inverts its pivots
+          else
+            am.a[rr][qq] = a;
         }
+        // N = 3: rows that the first level eliminates keep a^-1
+        if constexpr (N == 3) stm(row, ((r & 1) == 0 && 1 < nr) ? inv(am) : am);
         put_rhs(r);
       }
       for (int r0 = 0; r0 < nx1; r0 += nth) {
@@ -1073,7 +1088,9 @@ struct ColLaunch {
 
 inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double *w,
                        const double *du, const double *u, const double *u1, ColLaunch &cl) {
-  const ColSmem L = col_smem(nv, g.nc1, g.nx1, nimpl, per ? 1 : 0);
+  const int compact =
+      !per && (nimpl == 5 || (nimpl == 3 && kCompact3 && !g.shell)) ? 1 : 0;
+  const ColSmem L = col_smem(nv, g.nc1, g.nx1, nimpl, per ? 1 : 0, compact);
   cl.smem = sizeof(double) * (size_t)L.total;
   if (cl.smem > 227 * 1024) {
     set_error("x1 pencil too long for shared memory");
@@ -1085,7 +1102,7 @@ inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double 
   cl.nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)
                 ? g.col_threads
                 : kColThreads;
-  if (nimpl == 5 && !per) cl.nthr = kCol5Threads;
+  if (compact) cl.nthr = nimpl == 5 ? kCol5Threads : (cl.nthr < kCol3Threads ? cl.nthr : kCol3Threads);
   // bulk copies move whole pencil rows: 16-byte aligned bases and an even
   // row length keep every row 16-byte aligned
   auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };
