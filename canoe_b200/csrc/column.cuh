@@ -54,12 +54,20 @@ struct ColPlan {
   static constexpr int blocks = N == 5 ? (PER ? 1 : 2) : (compact ? 4 : 3);
 };
 
+// doubles per block row a | b | c | rhs (x after the solve), rounded up to
+// 1 mod 16; with one more double after every 16 rows (row r starts at
+// r ROW + r / 16) the rows a reduction level touches, 2s apart, fall in
+// distinct 8-byte shared-memory banks for s = 1, 2, 4, 8 (the padding of
+// Harris, Sengupta and Owens, GPU Gems 3 ch. 39, applied to whole rows)
+__host__ __device__ constexpr int col_row(int n) { return ((3 * n * n + n + 14) / 16) * 16 + 1; }
+__host__ __device__ constexpr int col_rows(int n, int nx1) {
+  return nx1 * col_row(n) + (nx1 >> 4) + 1;
+}
+
 template <int N>
 struct ColRow {
   static constexpr int NN = N * N;
-  // a | b | c | rhs (x after the solve), padded to an odd number of doubles
-  // so that neighbouring rows fall in different shared-memory banks
-  static constexpr int ROW = (3 * NN + N) | 1;
+  static constexpr int ROW = col_row(N);
 };
 
 // shared-memory plan (doubles) of one pencil
@@ -84,12 +92,12 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
     // (plus three blocks past the last row, at stg), and u / u1 are not
     // prefetched
     const int nn = n_impl * n_impl;
-    const int rows = even_up(nx1 * ((3 * nn + n_impl) | 1));
+    const int rows = even_up(col_rows(n_impl, nx1));
     s.stg = s.uni + rows;
     solve = rows + 3 * nn;
   } else if (n_impl) {
     const int nn = n_impl * n_impl;
-    const int rows = even_up(nx1 * ((3 * nn + n_impl) | 1));
+    const int rows = even_up(col_rows(n_impl, nx1));
     // |A| and J, later reused as the staging area of u and u1
     const int aj = (nx1 + 1) * nn + (nx1 + 2) * nn;
     const int st = 2 * nv * nc1;
@@ -465,7 +473,8 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
 
   if constexpr (N > 0) {
     constexpr int NN = ColRow<N>::NN, ROW = ColRow<N>::ROW;
-    double *blk = un;                        // [nx1][ROW]
+    double *blk = un;                        // [nx1][ROW] + r / 16 padding
+    auto RP = [&](int r) { return blk + r * ROW + (r >> 4); };  // row r
     double *sA = sm + L.stg;                 // [nx1+1][NN] |A| at faces is-1/2..ie+1/2
     double *sJ = sA + (nx1 + 1) * NN;        // [nx1+2][NN] J of cells is-1..ie+1
     // COMPACT (row-parallel 5x5): |A| at face t < nx1 sits in row t's c
@@ -473,11 +482,11 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     // at stg
     constexpr bool COMPACT = ColPlan<N, PER, GEO>::compact;
     auto pA = [&](int t) -> double * {
-      if constexpr (COMPACT) return t < nx1 ? blk + t * ROW + 2 * NN : sA;
+      if constexpr (COMPACT) return t < nx1 ? RP(t) + 2 * NN : sA;
       else return sA + t * NN;
     };
     auto pJ = [&](int t) -> double * {
-      if constexpr (COMPACT) return t < nx1 ? blk + t * ROW + NN : sA + (t - nx1 + 1) * NN;
+      if constexpr (COMPACT) return t < nx1 ? RP(t) + NN : sA + (t - nx1 + 1) * NN;
       else return sJ + t * NN;
     };
     const double gm1 = th.gammad - 1.;
@@ -566,7 +575,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       double r0 = dc[i];
 #pragma unroll
       for (int n = 1; n <= NY; ++n) r0 += dc[n * nc1 + i];
-      double *rh = blk + r * ROW + 3 * NN;
+      double *rh = RP(r) + 3 * NN;
       rh[0] = r0 / dt;
       rh[1] = dc[S::IVX * nc1 + i] / dt;
       if constexpr (N == 3) {
@@ -585,7 +594,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
         double aL, aR, i2v;
         row_geom(r, aL, aR, i2v);
         const double *Am = pA(r), *Ap = pA(r + 1), *Jm = pJ(r), *Jc = pJ(r + 1), *Jn = pJ(r + 2);
-        double *row = blk + r * ROW;
+        double *row = RP(r);
         M<N> am;
 #pragma unroll
         for (int e = 0; e < NN; ++e) {
@@ -628,7 +637,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
           }
           __syncthreads();
           if (on) {
-            double *row = blk + r * ROW;
+            double *row = RP(r);
 #pragma unroll
             for (int kk = 0; kk < N; ++kk) {
               row[NN + q * N + kk] = bv[kk];
@@ -642,7 +651,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       const int i = is + r;
       double aL, aR, i2v;
       row_geom(r, aL, aR, i2v);
-      double *row = blk + r * ROW;
+      double *row = RP(r);
       M<N> am;
 #pragma unroll
       for (int e = 0; e < NN; ++e) {
@@ -695,8 +704,8 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     // warp 0 alone.
     auto level = [&](int s, int m) {
       const int r = 2 * s * (m + 1) - 1;
-      double *row = blk + r * ROW;
-      const double *lo = blk + (r - s) * ROW;
+      double *row = RP(r);
+      const double *lo = RP(r - s);
       M<N> a = ld(row), b = ld(row + NN), c = ld(row + 2 * NN);
       V<N> rh = ldv(row + 3 * NN);
       // alpha = -b a_lo^-1
@@ -719,7 +728,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
         for (int e = 0; e < NN; ++e) zr.a[e / N][e % N] += t.a[e / N][e % N];
       }
       if (r + s < nr) {
-        const double *hi = blk + (r + s) * ROW;
+        const double *hi = RP(r + s);
         M<N> ga = mm(c, ld(hi));
 #pragma unroll
         for (int e = 0; e < NN; ++e) ga.a[e / N][e % N] = -ga.a[e / N][e % N];
@@ -748,13 +757,13 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     };
     auto back = [&](int s, int m) {
       const int r = s - 1 + 2 * s * m;
-      double *row = blk + r * ROW;
+      double *row = RP(r);
       V<N> rh = ldv(row + 3 * NN);
       M<N> zr;
       if constexpr (PER) zr = ld(zb + r * NN);
       if (r - s >= 0) {
         const M<N> bm = ld(row + NN);
-        V<N> t = mv(bm, ldv(blk + (r - s) * ROW + 3 * NN));
+        V<N> t = mv(bm, ldv(RP(r - s) + 3 * NN));
 #pragma unroll
         for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
         if constexpr (PER) {
@@ -765,7 +774,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       }
       if (r + s < nr) {
         const M<N> cm = ld(row + 2 * NN);
-        V<N> t = mv(cm, ldv(blk + (r + s) * ROW + 3 * NN));
+        V<N> t = mv(cm, ldv(RP(r + s) + 3 * NN));
 #pragma unroll
         for (int e = 0; e < N; ++e) rh.a[e] -= t.a[e];
         if constexpr (PER) {
@@ -786,7 +795,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       const unsigned smask = 0xFFu << (tid & 24);
       // the block of row r: its a replaced by a^-1 in place
       auto invert_row = [&](int r) {
-        double *row = blk + r * ROW;
+        double *row = RP(r);
         double ar[5], iv[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) ar[q] = row[gg * 5 + q];
@@ -797,8 +806,8 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       };
       auto level5 = [&](int s, int m) {
         const int r = 2 * s * (m + 1) - 1;
-        double *row = blk + r * ROW;
-        const double *lo = blk + (r - s) * ROW;
+        double *row = RP(r);
+        const double *lo = RP(r - s);
         double ar[5], br[5], cr[5], al[5], bn[5], cn[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -833,7 +842,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
           rh += t;
         }
         if (r + s < nr) {
-          const double *hi = blk + (r + s) * ROW;
+          const double *hi = RP(r + s);
           double ga[5];
 #pragma unroll
           for (int q = 0; q < 5; ++q) {
@@ -885,17 +894,17 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       };
       auto back5 = [&](int s, int m) {
         const int r = s - 1 + 2 * s * m;
-        double *row = blk + r * ROW;
+        double *row = RP(r);
         double t = row[3 * NN + gg];
         if (r - s >= 0) {
-          const double *x = blk + (r - s) * ROW + 3 * NN;
+          const double *x = RP(r - s) + 3 * NN;
           double u = 0.;
 #pragma unroll
           for (int k = 0; k < 5; ++k) u += row[NN + gg * 5 + k] * x[k];
           t -= u;
         }
         if (r + s < nr) {
-          const double *x = blk + (r + s) * ROW + 3 * NN;
+          const double *x = RP(r + s) + 3 * NN;
           double u = 0.;
 #pragma unroll
           for (int k = 0; k < 5; ++k) u += row[2 * NN + gg * 5 + k] * x[k];
@@ -917,7 +926,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       }
       // the last surviving row r = stop - 1 is decoupled
       if (seg == 0) {
-        double *row = blk + (stop - 1) * ROW;
+        double *row = RP(stop - 1);
         double ar[5], iv[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) ar[q] = row[gg * 5 + q];
@@ -953,7 +962,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
         }
         // the last surviving row r = stop - 1 is decoupled
         if (lane == 0) {
-          double *row = blk + (stop - 1) * ROW;
+          double *row = RP(stop - 1);
           M<N> ai = inv(ld(row));
           stm(row, ai);
           stv(row + 3 * NN, mv(ai, ldv(row + 3 * NN)));
@@ -975,12 +984,12 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       // rows 0..n-2 hold y and Z with x = y - Z x(n-1); row n-1:
       // (a - s Z0 - b Z(n-2)) x(n-1) = rhs - s y0 - b y(n-2)
       if (tid == 0) {
-        double *row = blk + (nx1 - 1) * ROW;
+        double *row = RP(nx1 - 1);
         const M<N> bl = ld(row + NN), sc = ld(row + 2 * NN);
         M<N> sch = ld(row);
         V<N> rh = ldv(row + 3 * NN);
         const M<N> t0 = mm(sc, ld(zb)), t1 = mm(bl, ld(zb + (nr - 1) * NN));
-        const V<N> v0 = mv(sc, ldv(blk + 3 * NN)), v1 = mv(bl, ldv(blk + (nr - 1) * ROW + 3 * NN));
+        const V<N> v0 = mv(sc, ldv(RP(0) + 3 * NN)), v1 = mv(bl, ldv(RP(nr - 1) + 3 * NN));
 #pragma unroll
         for (int e = 0; e < NN; ++e) sch.a[e / N][e % N] -= t0.a[e / N][e % N] + t1.a[e / N][e % N];
 #pragma unroll
@@ -988,9 +997,9 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
         stv(row + 3 * NN, mv(inv(sch), rh));
       }
       __syncthreads();
-      const V<N> xl = ldv(blk + (nx1 - 1) * ROW + 3 * NN);
+      const V<N> xl = ldv(RP(nx1 - 1) + 3 * NN);
       for (int r = tid; r < nr; r += nth) {
-        double *x = blk + r * ROW + 3 * NN;
+        double *x = RP(r) + 3 * NN;
         const V<N> t = mv(ld(zb + r * NN), xl);
 #pragma unroll
         for (int e = 0; e < N; ++e) x[e] -= t.a[e];
@@ -999,7 +1008,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     }
     // P7a: species correction (forward_backward.hpp:101-124) into dc
     for (int r = tid; r < nx1; r += nth) {
-      const double *x = blk + r * ROW + 3 * NN;
+      const double *x = RP(r) + 3 * NN;
       const int i = is + r;
       double dv[NV];
 #pragma unroll
