@@ -395,7 +395,7 @@ def c5_report(net, steps=5, warmup=2):
                      "sequential_ms_per_step": ms_seq,
                      "sequential_value": cells / (ms_seq * 1e-3),
                      "threads_per_pencil": {str(t): int((choice == t).sum())
-                                            for t in (64, 96, 128, 160)},
+                                            for t in (64, 96, 128, 160, 192, 256)},
                      "error_words": int(np.bitwise_or.reduce(np.array(errs)))}
         bt.close()
         for b in blocks:

@@ -666,8 +666,8 @@ int canoe_block_error_word(canoe_block_t b, uint32_t *bits) {
 
 int canoe_block_set_column_threads(canoe_block_t b, int threads) {
   if (!b) return CANOE_ERR_ARG;
-  if (threads != 0 && (threads < 64 || threads > kColThreads || threads % 32)) {
-    set_error("threads per x1 pencil must be a multiple of 32 in 64..160 (0: default)");
+  if (threads != 0 && (threads < 64 || threads > 256 || threads % 32)) {
+    set_error("threads per x1 pencil must be a multiple of 32 in 64..256 (0: default)");
     return CANOE_ERR_ARG;
   }
   b->g.col_threads = threads;
@@ -788,12 +788,12 @@ int canoe_batch_synchronize(canoe_batch_t q) {
 }
 
 // Per block, time steps with each candidate number of threads per x1
-// pencil (64, 96, 128, 160) and keep the fastest; the blocks' states, dt
+// pencil (64 .. 256) and keep the fastest; the blocks' states, dt
 // and counters are restored afterwards.  h_threads (may be NULL) receives
 // the choices.
 int canoe_batch_autotune(canoe_batch_t q, int32_t *h_threads) {
   if (!q) return CANOE_ERR_ARG;
-  static const int cand[4] = {64, 96, 128, 160};
+  static const int cand[] = {64, 96, 128, 160, 192, 256};
   cudaEvent_t e0, e1;
   CB_CUDA(cudaEventCreate(&e0));
   CB_CUDA(cudaEventCreate(&e1));

@@ -40,9 +40,12 @@ constexpr int kColThreads = 160;
 // the full 5x5 solve runs row-parallel (8-lane segments per block row-op),
 // 7 warps per pencil and two pencils per SM
 constexpr int kCol5Threads = 224;
-// the 3x3 solve with the compact plan: 4 warps per pencil, four per SM
+// the 3x3 solve with the compact plan: 4 warps per pencil by default (four
+// pencils per SM at 128 levels), up to 8 when a batch's autotuner picks them
+// for tall columns, whose shared memory allows fewer pencils per SM
 constexpr bool kCompact3 = true;
 constexpr int kCol3Threads = 128;
+constexpr int kCol3ThreadsMax = 256;
 
 // the compact shared-memory plan (|A| and J staged in the rows' own slots,
 // no u / u1 prefetch): the 5x5 solve, and the 3x3 one when kCompact3
@@ -50,8 +53,9 @@ template <int N, bool PER, int GEO>
 struct ColPlan {
   static constexpr bool compact = !PER && (N == 5 || (N == 3 && kCompact3 && !GEO));
   static constexpr int threads =
-      !compact ? kColThreads : (N == 5 ? kCol5Threads : kCol3Threads);
-  static constexpr int blocks = N == 5 ? (PER ? 1 : 2) : (compact ? 4 : 3);
+      !compact ? kColThreads : (N == 5 ? kCol5Threads : kCol3ThreadsMax);
+  // registers: 65536 / (threads x blocks) = 128 per thread for the 3x3 plans
+  static constexpr int blocks = N == 5 ? (PER ? 1 : 2) : (compact ? 2 : 3);
 };
 
 // doubles per block row a | b | c | rhs (x after the solve), rounded up to
@@ -1111,7 +1115,12 @@ inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double 
   cl.nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)
                 ? g.col_threads
                 : kColThreads;
-  if (compact) cl.nthr = nimpl == 5 ? kCol5Threads : (cl.nthr < kCol3Threads ? cl.nthr : kCol3Threads);
+  if (compact)
+    cl.nthr = nimpl == 5 ? kCol5Threads
+                         : (g.col_threads >= 64 && g.col_threads <= kCol3ThreadsMax &&
+                            g.col_threads % 32 == 0)
+                               ? g.col_threads
+                               : kCol3Threads;
   // bulk copies move whole pencil rows: 16-byte aligned bases and an even
   // row length keep every row 16-byte aligned
   auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };

@@ -52,7 +52,7 @@ def test_autotune_keeps_state_and_results():
     u0 = [b.conserved() for b in blocks]
     bt = Batch(blocks)
     choice = bt.autotune()
-    assert all(c in (64, 96, 128, 160) for c in choice)
+    assert all(c in (64, 96, 128, 160, 192, 256) for c in choice)
     for b, u in zip(blocks, u0):
         assert np.array_equal(b.conserved(), u)
     bt.step()
@@ -60,3 +60,26 @@ def test_autotune_keeps_state_and_results():
     bt.synchronize()
     for b, r in zip(blocks, ref):
         assert np.array_equal(b.conserved(), r)
+
+
+@pytest.mark.parametrize("flag", [1, 9])
+def test_column_threads_do_not_change_results(flag):
+    """Any thread count per x1 pencil gives the same bits (3x3: 64..256; the
+    5x5 solve always runs 224 threads)."""
+    import ctypes
+    from canoe_b200 import problems
+    from canoe_b200._abi import check, load
+    lib = load()
+    out = []
+    for nt in (0, 64, 160, 256):
+        p = problems.moist3d(nx1=40, nx2=12, nx3=8, x1max=5000.0, x2max=3000.0,
+                             x3max=2000.0, noise=0.5, implicit_flag=flag)
+        b = MeshBlock(p)
+        check(lib.canoe_block_set_column_threads(b.h, nt))
+        b.step(1.0)
+        b.step(1.0)
+        out.append(b.conserved())
+        assert b.error_word() == 0
+        b.close()
+    for o in out[1:]:
+        assert np.array_equal(o, out[0])
