@@ -54,6 +54,14 @@ __global__ void __launch_bounds__(256)
   const int64_t base = (DIR == 1 ? (int64_t)o * g.sk : (int64_t)o * g.nc1) + i;
 
   const double pref = PERT ? g.pref[iok ? i : g.is] : 0.;
+  // x3 adds to the du of the x2 pass: this thread's du values are loaded at
+  // entry so that their latency hides behind the reconstruction
+  double dpre[NV];
+  if (DIR == 2 && iok && ty < nd && blockDim.y >= TD) {
+    const int64_t off = base + (int64_t)(d0 + ty) * sd;
+#pragma unroll
+    for (int n = 0; n < NV; ++n) dpre[n] = du[n * g.sv + off];
+  }
   // P0: stage cells d0-3 .. d0+nd+2
   for (int c = ty; c < nd + 2 * NG; c += blockDim.y) {
     const int64_t off = base + (int64_t)(d0 - NG + c) * sd;
@@ -122,6 +130,8 @@ __global__ void __launch_bounds__(256)
                   (double)F[(n * (TD + 1) + c) * TI + tx]) * idx;
       if (DIR == 1)
         du[n * g.sv + off] = -(wght * d);  // x2 runs first: initialise du
+      else if (blockDim.y >= TD)
+        du[n * g.sv + off] = dpre[n] - wght * d;  // c == ty: the prefetched cell
       else
         du[n * g.sv + off] -= wght * d;
     }
