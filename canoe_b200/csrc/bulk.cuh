@@ -50,6 +50,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// start moving [src, src + bytes) into L2 (no completion to wait for; the
+// data is then read by ordinary loads); 16-byte aligned, bytes % 16 == 0
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *m, uint32_t parity) {
   uint32_t ok;
   asm volatile(

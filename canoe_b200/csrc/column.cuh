@@ -188,6 +188,14 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
         for (int n = 0; n < NV; ++n)
           bulk_g2s(dc + n * nc1, du + n * g.sv + base, row_bytes, mbar + 1);
       }
+      // the compact plans read u and u1 only at the register update: start
+      // moving their rows into L2 now
+      if constexpr (UPDATE && ColPlan<N, PER, GEO>::compact) {
+        for (int n = 0; n < NV; ++n) {
+          bulk_prefetch_l2(u + n * g.sv + base, row_bytes);
+          if (stage != 0) bulk_prefetch_l2(u1 + n * g.sv + base, row_bytes);
+        }
+      }
     }
     __syncthreads();
     if (!__syncthreads_and(mbar_wait(mbar, 0))) {
