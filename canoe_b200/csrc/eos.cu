@@ -426,13 +426,15 @@ __device__ __forceinline__ bool may_condense(const canoe_thermo_t &th, const dou
     for (int n = 1; n <= NY; ++n)
       if (n == 1 + v || n == ls || n == ss) fam += uc[n];
     const bool liquid = (ss < 0) || (ls >= 0 && tv >= th.t3[v]);
-    const double beta = liquid ? th.beta_l[v] : th.beta_s[v];
-    const double delta = liquid ? th.delta_l[v] : th.delta_s[v];
-    const double rv = th.rd * (1. + th.inv_mu_ratio_m1[v]);
-    const double ps =
-        th.p3[v] * exp(beta * (1. - th.t3[v] / tv) - delta * log(tv / th.t3[v]));
+    const float beta = float(liquid ? th.beta_l[v] : th.beta_s[v]);
+    const float delta = float(liquid ? th.delta_l[v] : th.delta_s[v]);
+    const float rv = float(th.rd * (1. + th.inv_mu_ratio_m1[v]));
+    // a heuristic with a 1e-3 margin: FP32 intrinsics (relative error ~1e-6)
+    // are ample and cost a fraction of the FP64 exp / log
+    const float r = float(th.t3[v] / tv);
+    const float ps = float(th.p3[v]) * __expf(beta * (1.f - r) + delta * __logf(r));
     // vapour density of the family against saturation, with a 1e-3 margin
-    any = any || !(fam * rv * tv < (1. - 1e-3) * ps);
+    any = any || !(float(fam) * rv * float(tv) < (1.f - 1e-3f) * ps);
   }
   return any;
 }
@@ -451,16 +453,6 @@ __global__ void __launch_bounds__(256)
   __shared__ float sw1[LEARNED ? kMlpH * kMlpIn : 1], sb1[LEARNED ? kMlpH : 1],
       sb2[LEARNED ? kMlpH : 1], sw3[LEARNED ? kMlpH : 1];
   __shared__ __align__(16) __nv_bfloat16 sw2[LEARNED ? kMlpH * kMlpH : 2];
-  if constexpr (LEARNED) {
-    for (int q = threadIdx.x; q < kMlpH * kMlpIn; q += blockDim.x) sw1[q] = mv.p[kMlpOffW1 + q];
-    for (int q = threadIdx.x; q < kMlpH; q += blockDim.x) {
-      sb1[q] = mv.p[kMlpOffB1 + q];
-      sb2[q] = mv.p[kMlpOffB2 + q];
-      sw3[q] = mv.p[kMlpOffW3 + q];
-    }
-    for (int q = threadIdx.x; q < kMlpH * kMlpH; q += blockDim.x) sw2[q] = mv.w2h[q];
-    __syncthreads();
-  }
   int64_t off = t;
   double uc[S::NV];
   if (active) {
@@ -485,7 +477,20 @@ __global__ void __launch_bounds__(256)
       need = may_condense<NY>(th, uc, tdry);
     }
     tg = __longlong_as_double(0x7ff8000000000000LL);  // no guess: cold start
-    if (__any_sync(0xffffffffu, need)) {
+    // the network's weights go to shared memory only for a CTA that has a
+    // cell near saturation (every thread reaches this barrier)
+    const bool cta_need = __syncthreads_or(need);
+    if (cta_need) {
+      for (int q = threadIdx.x; q < kMlpH * kMlpIn; q += blockDim.x) sw1[q] = mv.p[kMlpOffW1 + q];
+      for (int q = threadIdx.x; q < kMlpH; q += blockDim.x) {
+        sb1[q] = mv.p[kMlpOffB1 + q];
+        sb2[q] = mv.p[kMlpOffB2 + q];
+        sw3[q] = mv.p[kMlpOffW3 + q];
+      }
+      for (int q = threadIdx.x; q < kMlpH * kMlpH; q += blockDim.x) sw2[q] = mv.w2h[q];
+      __syncthreads();
+    }
+    if (cta_need && __any_sync(0xffffffffu, need)) {
 #pragma unroll
       for (int q = 0; q < kMlpIn; ++q)
         x[q] = active ? (x[q] - mv.in_mean[q]) * mv.in_istd[q] : 0.f;
