@@ -35,6 +35,11 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// one plain arrival on mbarrier m
+__device__ __forceinline__ void mbar_arrive(uint64_t *m) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(m)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)),
                "r"(bytes)
@@ -68,9 +73,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *m, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait for phase `parity` of mbarrier m
-__device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t parity) {
-  for (int it = 0; it < kBulkSpin; ++it)
+// bounded wait for phase `parity` of mbarrier m: false after `spins` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t parity, int spins = kBulkSpin) {
+  for (int it = 0; it < spins; ++it)
     if (mbar_try_wait(m, parity)) return true;
   return false;
 }

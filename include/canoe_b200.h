@@ -150,6 +150,14 @@ const char *canoe_version(void);
 const char *canoe_last_error(void);
 int canoe_device_sm_count(int *out);
 
+/* Self-test of the bounded waits that guard the kernels' bulk copies: one
+ * thread waits at most `spins` polls for an mbarrier phase that is complete
+ * (complete != 0) or cannot complete before the wait (complete == 0), and
+ * *h_bits receives CANOE_EBIT_TIMEOUT if the wait gave up.  The kernel then
+ * completes the phase itself, so nothing stays pending.  No reference
+ * counterpart (the reference has no device waits). */
+int canoe_selftest_bounded_wait(int spins, int complete, uint32_t *h_bits);
+
 /* ---------------- operator-level entry points (device pointers) --------- */
 
 /* Hydro::RiemannSolver, LMARS: canoe src/snap/riemann/lmars.cpp:19-85.
