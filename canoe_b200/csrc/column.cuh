@@ -51,7 +51,7 @@ constexpr int kCol3ThreadsMax = 256;
 // no u / u1 prefetch): the 5x5 solve, and the 3x3 one when kCompact3
 template <int N, bool PER, int GEO>
 struct ColPlan {
-  static constexpr bool compact = !PER && (N == 5 || (N == 3 && kCompact3 && !GEO));
+  static constexpr bool compact = !PER && (N == 5 || (N == 3 && kCompact3));
   static constexpr int threads =
       !compact ? kColThreads : (N == 5 ? kCol5Threads : kCol3ThreadsMax);
   // registers: 65536 / (threads x blocks) = 128 per thread for the 3x3 plans
@@ -1110,7 +1110,7 @@ struct ColLaunch {
 inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double *w,
                        const double *du, const double *u, const double *u1, ColLaunch &cl) {
   const int compact =
-      !per && (nimpl == 5 || (nimpl == 3 && kCompact3 && !g.shell)) ? 1 : 0;
+      !per && (nimpl == 5 || (nimpl == 3 && kCompact3)) ? 1 : 0;
   const ColSmem L = col_smem(nv, g.nc1, g.nx1, nimpl, per ? 1 : 0, compact);
   cl.smem = sizeof(double) * (size_t)L.total;
   if (cl.smem > 227 * 1024) {
