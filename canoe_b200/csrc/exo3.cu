@@ -527,6 +527,14 @@ __global__ void __launch_bounds__(256)
   const int64_t base = (DIR == 1 ? (int64_t)o * g.sk : (int64_t)o * g.nc1) + i;
   const int64_t nkj = (int64_t)g.nc3 * g.nc2;
   const double pref = PERT ? g.pref[iok ? i : g.is] : 0.;
+  // x3 adds to the du of the x2 pass: this thread's du values are loaded at
+  // entry so that their latency hides behind the reconstruction
+  double dpre[kNV];
+  if (DIR == 2 && iok && ty < nd && blockDim.y >= TD) {
+    const int64_t off = pb + base + (int64_t)(d0 + ty) * sd;
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) dpre[n] = du[n * g.sv + off];
+  }
   for (int c = ty; c < nd + 2 * NG; c += blockDim.y) {
     const int64_t off = pb + base + (int64_t)(d0 - NG + c) * sd;
 #pragma unroll
@@ -670,6 +678,8 @@ __global__ void __launch_bounds__(256)
       const double dfl = ap * F[n][c + 1][tx] - am * F[n][c][tx];
       if (DIR == 1)
         du[n * g.sv + off] = -(wght * dfl / vol);
+      else if (blockDim.y >= TD)
+        du[n * g.sv + off] = dpre[n] - wght * dfl / vol;  // c == ty: the prefetched cell
       else
         du[n * g.sv + off] -= wght * dfl / vol;
     }
