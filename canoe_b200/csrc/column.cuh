@@ -1123,12 +1123,16 @@ inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double 
   cl.nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)
                 ? g.col_threads
                 : kColThreads;
+  // compact 3x3 default: one thread per level rounded up to a warp, between
+  // 2 and 4 warps.  Short columns need little shared memory, so the register
+  // file sets the pencils per SM: at 64 levels eight pencils of 2 warps run
+  // where four of 4 warps would
   if (compact)
     cl.nthr = nimpl == 5 ? kCol5Threads
                          : (g.col_threads >= 64 && g.col_threads <= kCol3ThreadsMax &&
                             g.col_threads % 32 == 0)
                                ? g.col_threads
-                               : kCol3Threads;
+                               : min(max((g.nx1 + 31) / 32 * 32, 64), kCol3Threads);
   // bulk copies move whole pencil rows: 16-byte aligned bases and an even
   // row length keep every row 16-byte aligned
   auto al16 = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };
