@@ -342,8 +342,9 @@ int canoe_block_satadj_stats(canoe_block_t b, unsigned long long *h_stats);
 int canoe_block_error_word(canoe_block_t b, uint32_t *bits);
 
 /* Threads per x1 pencil (CTA of the column kernel): a multiple of 32 in
- * 64..256, 0 for the default (128 with the 3x3 implicit solve, 224 with the
- * 5x5 one, 160 otherwise).  Kernels without the 3x3 solve use at most 160
+ * 64..256, 0 for the default (with the 3x3 implicit solve the column height
+ * rounded up to a multiple of 32, within 64..128; 224 with the 5x5 solve;
+ * 160 otherwise).  Kernels without the 3x3 solve use at most 160
  * and the 5x5 solve always 224.  Results do not depend on it.  No reference
  * counterpart (the reference sweeps columns serially). */
 int canoe_block_set_column_threads(canoe_block_t b, int threads);
