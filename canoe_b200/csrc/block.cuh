@@ -37,6 +37,10 @@ struct Geom {
   // threads per x1 pencil (a multiple of 32 in 64..160; 0 = 160), chosen
   // per block by canoe_batch_autotune
   int col_threads;
+  // x1 pencil launches over npanel equal blocks stored pstride doubles apart
+  // (the six panels of a cubed-sphere shell share one geometry)
+  int npanel = 1;
+  int64_t pstride = 0;
 };
 
 // geometry tables of a cubed-sphere panel (gnomonic_equiangle.cpp:140-222)

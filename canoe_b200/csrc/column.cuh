@@ -152,9 +152,18 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
   double *un = sm + L.uni;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + L.mbar);
 
-  const int j = g.js + (int)(blockIdx.x % (unsigned)g.nx2);
-  const int k = g.ks + (int)(blockIdx.x / (unsigned)g.nx2);
+  const unsigned ncol = (unsigned)g.nx2 * (unsigned)g.nx3;
+  const unsigned col = blockIdx.x % ncol;
+  const int j = g.js + (int)(col % (unsigned)g.nx2);
+  const int k = g.ks + (int)(col / (unsigned)g.nx2);
   const int64_t base = (int64_t)k * g.sk + (int64_t)j * nc1;
+  if (g.npanel > 1) {  // panel of this column: shift the block arrays
+    const int64_t poff = (int64_t)(blockIdx.x / ncol) * g.pstride;
+    w += poff;
+    du += poff;
+    u += poff;
+    u1 += poff;
+  }
   const int tid = threadIdx.x, nth = blockDim.x;
   const int warp = tid >> 5, lane = tid & 31;
   // panel geometry of the column (GEO)
@@ -1117,7 +1126,7 @@ inline int col_prepare(const Geom &g, int nv, int nimpl, bool per, const double 
     set_error("x1 pencil too long for shared memory");
     return CANOE_ERR_UNSUPPORTED;
   }
-  cl.nblk = (unsigned)g.nx2 * (unsigned)g.nx3;
+  cl.nblk = (unsigned)g.nx2 * (unsigned)g.nx3 * (unsigned)(g.npanel > 1 ? g.npanel : 1);
   // threads per pencil: the kernel strides every loop by blockDim and needs
   // at least two warps (warp 0 runs the scan while the others reconstruct)
   cl.nthr = (g.col_threads >= 64 && g.col_threads <= kColThreads && g.col_threads % 32 == 0)

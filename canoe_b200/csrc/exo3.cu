@@ -989,13 +989,15 @@ int canoe_shell_step(canoe_shell_t s, double dt) {
     if ((rc = shell_edges(s))) return rc;
     if ((rc = shell_x23(s, 1, sg.beta, nullptr))) return rc;
     if ((rc = shell_x23(s, 2, sg.beta, nullptr))) return rc;
-    for (int p = 0; p < 6; ++p)
-      if ((rc = launch_x1col(s->g, s->th, s->cfg.recon, s->cfg.rsolver, s->cfg.implicit_flag,
-                             s->cfg.precision, kColStep, s->d_w + p * s->pvals,
-                             s->d_du + p * s->pvals,
-                             s->d_u + p * s->pvals, s->d_u1 + p * s->pvals, s->d_dt, sg, stage,
-                             nullptr, s->st)))
+    {  // the six panels' x1 pencils in one launch
+      Geom g6 = s->g;
+      g6.npanel = 6;
+      g6.pstride = s->pvals;
+      if ((rc = launch_x1col(g6, s->th, s->cfg.recon, s->cfg.rsolver, s->cfg.implicit_flag,
+                             s->cfg.precision, kColStep, s->d_w, s->d_du, s->d_u, s->d_u1,
+                             s->d_dt, sg, stage, nullptr, s->st)))
         return rc;
+    }
     if ((rc = shell_ghosts(s))) return rc;
     if ((rc = shell_c2p(s))) return rc;
   }
