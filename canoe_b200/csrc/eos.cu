@@ -440,7 +440,7 @@ __device__ __forceinline__ bool may_condense(const canoe_thermo_t &th, const dou
 }
 
 template <int NY, bool LEARNED>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     k_satadj(canoe_thermo_t th, canoe_satadj_opts_t o, double *__restrict__ u,
              int64_t ncells, int64_t stride, Geom g, int use_geom,
              const double *__restrict__ t_guess, double *__restrict__ t_out,
