@@ -25,8 +25,9 @@ constexpr int TD = 8;   // tile length along the flux direction
 // R = double: the FP64 path.  R = float: reconstruction and Riemann fluxes
 // in FP32 on p' = p - pref(i); pref is the same on both sides of an x2 / x3
 // face, so it cancels from the momentum-flux divergence exactly.
+// FP32 tiles: four CTAs per SM (64 registers); FP64: three
 template <int NY, int RECON, int RS, int DIR, bool WF, typename R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3)
     k_flux_x23(Geom g, canoe_thermo_t th, const double *__restrict__ w,
                double *__restrict__ du, const double *__restrict__ dtp,
                double beta, double *__restrict__ fout) {
