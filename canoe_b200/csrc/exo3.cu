@@ -497,8 +497,9 @@ constexpr int TI = 32, TD = 8;
 // projection and the divergence stay FP64, with pref added back to the
 // normal momentum flux before them (the transforms mix it into the
 // transverse components, and face areas differ across a cell).
+// FP32 tiles: four CTAs per SM (64 registers); FP64: two
 template <int RECON, int DIR, bool WF, typename R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
     k_shell_flux_x23(Geom g, canoe_thermo_t th, const double *__restrict__ w,
                      double *__restrict__ du, const double *__restrict__ dtp, double beta,
                      int64_t pvals, const double *__restrict__ lr, double *__restrict__ fout) {
