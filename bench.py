@@ -653,6 +653,16 @@ def main():
     f5 = None
     if rank == 0 and not args.no_5x5:
         f5 = full5x5_report(args, net)
+    fma = None
+    if rank == 0:
+        # non-tensor FMA peaks of this GPU (outside every timed region): the
+        # denominator for the x1 pencil's FP64 arithmetic in profiles/
+        p64, p32 = ctypes.c_double(0.), ctypes.c_double(0.)
+        check(lib.canoe_measure_fma_peak(0, ctypes.byref(p64)))
+        check(lib.canoe_measure_fma_peak(1, ctypes.byref(p32)))
+        fma = {"fp64_tflops": p64.value, "fp32_tflops": p32.value,
+               "how": "8 independent FMA chains per thread, 8 CTAs x 256 threads per SM, "
+                      "CUDA events after a warm-up launch"}
     if rank == 0 and not args.no_c4:
         c4 = c4_report(net, p.cfg.thermo)
     if dist:
@@ -673,6 +683,7 @@ def main():
             "c3_cubed_sphere_shell": c3,
             "c5_batched_blocks": c5,
             "c2_full5x5": f5,
+            "fma_peaks": fma,
             "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
             "error_word": err}
     print(json.dumps(line), flush=True)

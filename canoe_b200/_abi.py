@@ -108,6 +108,7 @@ SIGNATURES = [
     ("canoe_mlp_forward", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
     ("canoe_block_set_column_threads", c_int, [c_void_p, c_int]),
     ("canoe_selftest_bounded_wait", c_int, [c_int, c_int, c_void_p]),
+    ("canoe_measure_fma_peak", c_int, [c_int, POINTER(c_double)]),
     ("canoe_batch_create", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     ("canoe_batch_destroy", c_int, [c_void_p]),
     ("canoe_batch_use_graph", c_int, [c_void_p, c_int]),

@@ -42,3 +42,65 @@ extern "C" int canoe_selftest_bounded_wait(int spins, int complete, uint32_t *h_
   CB_CUDA(e);
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Non-tensor FMA throughput of this GPU (the denominator for FP64 / FP32
+// arithmetic): eight independent fused multiply-add chains per thread on
+// every SM, long enough that launch overhead is negligible.
+
+namespace cb {
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_peak(T *out, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) x[c] = T(threadIdx.x + c) * T(1e-3);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x[c] = fma(x[c], a, b);
+  }
+  T s = x[0];
+#pragma unroll
+  for (int c = 1; c < 8; ++c) s += x[c];
+  if (s == T(-1)) out[blockIdx.x] = s;  // keeps the chains live; never true
+}
+
+template <typename T>
+int fma_peak(int iters, double *tflops) {
+  int dev = 0, nsm = 0;
+  CB_CUDA(cudaGetDevice(&dev));
+  CB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int grid = nsm * 8, threads = 256;
+  T *d = nullptr;
+  CB_CUDA(cudaMalloc(&d, grid * sizeof(T)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const T a = T(0.999999), b = T(1e-7);
+  k_fma_peak<T><<<grid, threads>>>(d, iters / 8, a, b);  // warm-up
+  cudaEventRecord(e0);
+  k_fma_peak<T><<<grid, threads>>>(d, iters, a, b);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  CB_CUDA(e);
+  *tflops = 2.0 * 8.0 * (double)iters * grid * threads / (ms * 1e-3) / 1e12;
+  return 0;
+}
+
+}  // namespace
+}  // namespace cb
+
+extern "C" int canoe_measure_fma_peak(int fp32, double *h_tflops) {
+  using namespace cb;
+  if (!h_tflops) {
+    set_error("canoe_measure_fma_peak: null result pointer");
+    return CANOE_ERR_ARG;
+  }
+  return fp32 ? fma_peak<float>(1 << 17, h_tflops) : fma_peak<double>(1 << 14, h_tflops);
+}

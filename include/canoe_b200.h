@@ -158,6 +158,12 @@ int canoe_device_sm_count(int *out);
  * counterpart (the reference has no device waits). */
 int canoe_selftest_bounded_wait(int spins, int complete, uint32_t *h_bits);
 
+/* Measured non-tensor FMA throughput of the current GPU in TFLOP/s (2 flops
+ * per FMA): FP64 (fp32 == 0) or FP32, eight independent chains per thread on
+ * every SM, timed with CUDA events after a warm-up launch.  The denominator
+ * the bench uses for FP64 / FP32 arithmetic.  No reference counterpart. */
+int canoe_measure_fma_peak(int fp32, double *h_tflops);
+
 /* ---------------- operator-level entry points (device pointers) --------- */
 
 /* Hydro::RiemannSolver, LMARS: canoe src/snap/riemann/lmars.cpp:19-85.
