@@ -123,10 +123,13 @@ __host__ __device__ inline ColSmem col_smem(int nv, int nc1, int nx1, int n_impl
 //
 // Latency hiding inside the CTA: the pencil rows of w and du arrive by bulk
 // copies issued at entry; u and u1 are fetched into the dead |A| / J area
-// while the cyclic reduction runs; the serial hydrostatic scan (one lane of
-// warp 0) overlaps the reconstruction of the variables it does not touch.
+// while the cyclic reduction runs (plans with a separate |A| / J area), or,
+// in the compact plans, moved into L2 by bulk prefetches issued at entry;
+// the serial hydrostatic scan (one lane of warp 0) overlaps the
+// reconstruction of the variables it does not touch.
 //
-// GEO = 1: a cubed-sphere panel (dry, FP64, HLLC): covariant kinetic energy
+// GEO = 1: a cubed-sphere panel (dry, HLLC, FP64 or FP32 fluxes; the six
+// panels of a shell in one launch through Geom::npanel): covariant kinetic energy
 // in the Riemann problem and the covariant flux projection
 // (hllc_transform.cpp:92-101, 245-272), radial face areas and cell volumes
 // (gnomonic_equiangle.cpp:224-432), the coordinate source terms
