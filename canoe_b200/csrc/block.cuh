@@ -115,6 +115,10 @@ int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                   const MlpView *mlp = nullptr, double *guess_out = nullptr);
 MlpView mlp_view(const struct canoe_mlp *m);
 
+// all checks a block configuration passes before a step runs on it (capi.cu);
+// 0 or a canoe_status with the message set
+int validate_block_config(const canoe_block_config_t &c);
+
 // raise a kernel's dynamic shared-memory limit once per (kernel, size)
 int ensure_smem(const void *kernel, size_t bytes);
 

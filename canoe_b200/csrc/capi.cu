@@ -150,6 +150,57 @@ struct canoe_block {
   size_t nvals = 0;
 };
 
+// Every check a block configuration must pass before a step may run on it
+// (shared by canoe_block_create and canoe_block_step_noalloc, so that the two
+// entry points accept exactly the same configurations).
+namespace cb {
+int validate_block_config(const canoe_block_config_t &c) {
+  if (int rc = check_thermo(c.thermo)) return rc;
+  if (c.nx1 < 4 || c.nx2 < 1 || c.nx3 < 1 || !c.h_x1f) {
+    set_error("block needs nx1 >= 4, nx2, nx3 >= 1 and x1 faces");
+    return CANOE_ERR_ARG;
+  }
+  if (c.nx3 > 1 && c.nx2 == 1) {
+    set_error("a 3-D block needs nx2 > 1");
+    return CANOE_ERR_ARG;
+  }
+  if (c.recon != CANOE_RECON_PLM && c.recon != CANOE_RECON_PPM) {
+    set_error("recon must be 2 (PLM) or 3 (PPM)");
+    return CANOE_ERR_ARG;
+  }
+  if (c.rsolver != CANOE_RSOLVER_LMARS && c.rsolver != CANOE_RSOLVER_HLLC) {
+    set_error("unknown Riemann solver");
+    return CANOE_ERR_ARG;
+  }
+  if (c.precision != CANOE_FP64 && c.precision != CANOE_FP32_PERTURBATION) {
+    set_error("precision must be CANOE_FP64 or CANOE_FP32_PERTURBATION");
+    return CANOE_ERR_ARG;
+  }
+  if ((((c.implicit_flag & 2) && c.nx2 > 1) || ((c.implicit_flag & 4) && c.nx3 > 1)) &&
+      c.thermo.ny > 0) {
+    // the reference's moist x2 / x3 update reads w at the transposed
+    // indices (forward_backward.hpp:107-110 under solve_implicit_3d.cpp:
+    // 35-89), i.e. at unrelated cells
+    set_error("x2 / x3 implicit solves are provided for a dry block");
+    return CANOE_ERR_UNSUPPORTED;
+  }
+  for (int i = 0; i < c.nx1; ++i)
+    if (!(c.h_x1f[i + 1] > c.h_x1f[i])) {
+      set_error("x1 faces must increase");
+      return CANOE_ERR_ARG;
+    }
+  if (c.recon == CANOE_RECON_PPM) {
+    double d0 = c.h_x1f[1] - c.h_x1f[0];
+    for (int i = 1; i < c.nx1; ++i)
+      if (std::fabs((c.h_x1f[i + 1] - c.h_x1f[i]) - d0) > 1e-9 * d0) {
+        set_error("PPM needs a uniform x1 grid");
+        return CANOE_ERR_UNSUPPORTED;
+      }
+  }
+  return 0;
+}
+}  // namespace cb
+
 static int block_free(canoe_block *b) {
   if (!b) return 0;
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -305,48 +356,7 @@ int canoe_block_create(const canoe_block_config_t *cfg, canoe_block_t *out) {
     return CANOE_ERR_ARG;
   }
   *out = nullptr;
-  if (int rc = check_thermo(cfg->thermo)) return rc;
-  if (cfg->nx1 < 4 || cfg->nx2 < 1 || cfg->nx3 < 1 || !cfg->h_x1f) {
-    set_error("block needs nx1 >= 4, nx2, nx3 >= 1 and x1 faces");
-    return CANOE_ERR_ARG;
-  }
-  if (cfg->nx3 > 1 && cfg->nx2 == 1) {
-    set_error("a 3-D block needs nx2 > 1");
-    return CANOE_ERR_ARG;
-  }
-  if (cfg->recon != CANOE_RECON_PLM && cfg->recon != CANOE_RECON_PPM) {
-    set_error("recon must be 2 (PLM) or 3 (PPM)");
-    return CANOE_ERR_ARG;
-  }
-  if (cfg->rsolver != CANOE_RSOLVER_LMARS && cfg->rsolver != CANOE_RSOLVER_HLLC) {
-    set_error("unknown Riemann solver");
-    return CANOE_ERR_ARG;
-  }
-  if (cfg->precision != CANOE_FP64 && cfg->precision != CANOE_FP32_PERTURBATION) {
-    set_error("precision must be CANOE_FP64 or CANOE_FP32_PERTURBATION");
-    return CANOE_ERR_ARG;
-  }
-  if ((((cfg->implicit_flag & 2) && cfg->nx2 > 1) || ((cfg->implicit_flag & 4) && cfg->nx3 > 1)) &&
-      cfg->thermo.ny > 0) {
-    // the reference's moist x2 / x3 update reads w at the transposed
-    // indices (forward_backward.hpp:107-110 under solve_implicit_3d.cpp:
-    // 35-89), i.e. at unrelated cells
-    set_error("x2 / x3 implicit solves are provided for a dry block");
-    return CANOE_ERR_UNSUPPORTED;
-  }
-  for (int i = 0; i < cfg->nx1; ++i)
-    if (!(cfg->h_x1f[i + 1] > cfg->h_x1f[i])) {
-      set_error("x1 faces must increase");
-      return CANOE_ERR_ARG;
-    }
-  if (cfg->recon == CANOE_RECON_PPM) {
-    double d0 = cfg->h_x1f[1] - cfg->h_x1f[0];
-    for (int i = 1; i < cfg->nx1; ++i)
-      if (std::fabs((cfg->h_x1f[i + 1] - cfg->h_x1f[i]) - d0) > 1e-9 * d0) {
-        set_error("PPM needs a uniform x1 grid");
-        return CANOE_ERR_UNSUPPORTED;
-      }
-  }
+  if (int rc = validate_block_config(*cfg)) return rc;
   canoe_block *b = new canoe_block();
   b->cfg = *cfg;
   b->cfg.h_x1f = nullptr;

@@ -86,12 +86,10 @@ extern "C" int canoe_block_step_noalloc(const canoe_block_config_t *cfg, double 
     set_error("canoe_block_step_noalloc: null pointer or non-positive dt");
     return CANOE_ERR_ARG;
   }
+  // the same checks as canoe_block_create: a configuration it refuses is
+  // refused here too
+  if (int rc = validate_block_config(*cfg)) return rc;
   const canoe_thermo_t &th = cfg->thermo;
-  if (th.ny < 0 || th.ny > CANOE_MAX_NY || th.nvapor < 0 || th.nvapor > th.ny ||
-      cfg->nx1 < 4 || cfg->nx2 < 1 || cfg->nx3 < 1 || (cfg->nx3 > 1 && cfg->nx2 == 1)) {
-    set_error("canoe_block_step_noalloc: invalid block configuration");
-    return CANOE_ERR_ARG;
-  }
   const cudaStream_t st = (cudaStream_t)stream;
   Geom g{};
   g.ny = th.ny;

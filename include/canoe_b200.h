@@ -285,8 +285,7 @@ int canoe_block_step(canoe_block_t b, double dt);
  * callers that cannot let a library allocate device memory while they run
  * (a host model whose memory pool holds the GPU's memory, where a cudaMalloc
  * would fail or synchronize the device inside its own time step).  No
- * counterpart in the reference (its MeshBlock owns its arrays,
- * src/interface/hydro.hpp:54-67).
+ * counterpart in the reference.
  *   cfg   block configuration as for canoe_block_create
  *   d_u   device conserved state (NV, nc3, nc2, nc1), ghosts included:
  *         read, advanced by dt in place
@@ -299,8 +298,14 @@ int canoe_block_step(canoe_block_t b, double dt);
  * The step's other arrays (du, u1, geometry, dt) live in one fixed device
  * array of 16 MiB (2 Mi doubles) per device, which must hold
  * 2 NV nc3 nc2 nc1 + 4 nc1 + 8 doubles: larger blocks return CANOE_ERR_ARG.
- * The first call on a device looks up that array's address; make it before
- * any stream capture begins.  All calls on a device share the array, so
+ * The configuration is checked exactly as canoe_block_create checks it.
+ * The first call on a device looks up that array's address.  With CUDA's
+ * lazy module loading that first call is also when the library's module is
+ * loaded onto the device and the 16 MiB array takes its device memory, so a
+ * caller makes one call (a warm-up step on a scratch state is enough) at
+ * set-up, before it hands the GPU's free memory to its own pool; later
+ * calls allocate nothing.  h_x1f is copied to the device on every call
+ * from the caller's host memory.  All calls on a device share the array, so
  * calls that overlap in time (other streams or threads) race and corrupt
  * each other's results: order them on one stream.  The saturation
  * adjustment (cfg->satadj) uses the cold start.  X2 / X3 implicit solves
