@@ -121,6 +121,30 @@ int oracle_block_step(void *h, double dt, int nsteps) {
 
 double oracle_block_new_dt(void *h) { return oracle::new_dt(*static_cast<Block *>(h)); }
 
+// The x1 hydrostatic decomposition of column (k, j) of the block's primitive
+// state: q (nv x nc1) receives the decomposed pencil (T, p'), psf (nc1 + 1),
+// psv and gam (nc1) the column's hydrostatic arrays.
+int oracle_x1_change_to_temperature(void *h, int k, int j, double *q, double *psf,
+                                    double *psv, double *gam) {
+  Block &b = *static_cast<Block *>(h);
+  for (int n = 0; n < b.nv; ++n)
+    for (int i = 0; i < b.nc1; ++i) q[n * b.nc1 + i] = b.w[b.idx(n, k, j, i)];
+  oracle::change_to_temperature_pencil(b, k, j, q);
+  std::memcpy(psf, &b.psf[((size_t)k * b.nc2 + j) * (b.nc1 + 1)], (b.nc1 + 1) * sizeof(double));
+  std::memcpy(psv, &b.psv[b.idx(0, k, j, 0)], b.nc1 * sizeof(double));
+  std::memcpy(gam, &b.gam[b.idx(0, k, j, 0)], b.nc1 * sizeof(double));
+  return 0;
+}
+
+// Its inverse with the column's arrays of the last call above: q back to rho
+// and p, face states wl / wr (nv x (nc1 + 1)) of faces lo..hi restored.
+int oracle_x1_restore_from_temperature(void *h, int k, int j, double *q, double *wl,
+                                       double *wr, int lo, int hi) {
+  Block &b = *static_cast<Block *>(h);
+  oracle::restore_from_temperature_pencil(b, k, j, q, wl, wr, lo, hi);
+  return 0;
+}
+
 int oracle_riemann(int rsolver, const canoe_thermo_t *th, int ivx,
                    const double *wl, const double *wr, double *flx, int64_t n) {
   if (rsolver == CANOE_RSOLVER_LMARS)

@@ -456,55 +456,93 @@ static void riemann(const Block &b, int ivx, const double *wl, const double *wr,
     riemann_hllc(b.th, ivx, wl, wr, flx, n);
 }
 
+// Decomposition::ChangeToTemperature for column (k, j)
+// (change_to_temperature.cpp:40-136): fills the block's psf / psv / gamma_
+// for the column and turns the pencil q(n, i) (nv x nc1) into T and p'.
+void change_to_temperature_pencil(Block &b, int k, int j, double *q) {
+  const int nc1 = b.nc1, ipr = b.ipr;
+  const int is = b.is, ie = b.ie;
+  const double grav = b.th.grav;
+  if (grav == 0.) return;
+  double *psf = &b.psf[((size_t)k * b.nc2 + j) * (nc1 + 1)];
+  double *psv = &b.psv[b.idx(0, k, j, 0)];
+  double *gam = &b.gam[b.idx(0, k, j, 0)];
+  double *rho = &q[0], *pre = &q[ipr * nc1];
+  // change_to_temperature.cpp:57-64 isothermal extrapolation to the top
+  double RdTv = pre[ie] / rho[ie];
+  psf[ie + 1] = pre[ie] * std::exp(grav * b.dx1f[ie] / (2 * RdTv));
+  // :65 IntegrateDownwards (:30-38)
+  for (int i = ie; i >= is; --i) psf[i] = psf[i + 1] - grav * rho[i] * b.dx1f[i];
+  // :71-82 ghost psf, reflecting walls integrate with -grav
+  double gb = b.cfg.bc[0] == CANOE_BC_REFLECT ? -grav : grav;
+  for (int i = is - 1; i >= is - NG; --i) psf[i] = psf[i + 1] - gb * rho[i] * b.dx1f[i];
+  double gt = b.cfg.bc[1] == CANOE_BC_REFLECT ? -grav : grav;
+  for (int i = ie + 1; i <= ie + NG; ++i) psf[i + 1] = psf[i] + gt * rho[i] * b.dx1f[i];
+  // :89-111 per cell: log-mean psv, RovRd, rho -> T, p -> p'
+  for (int i = is - NG; i <= ie + NG; ++i) {
+    if (std::fabs(psf[i] - psf[i + 1]) < 1.E-6)
+      psv[i] = 0.5 * (psf[i] + psf[i + 1]);
+    else
+      psv[i] = (psf[i] - psf[i + 1]) / std::log(psf[i] / psf[i + 1]);
+    double feps = 1.;
+    for (int n = 1; n <= b.th.nvapor; ++n)
+      feps += q[n * nc1 + i] * b.th.inv_mu_ratio_m1[n - 1];
+    gam[i] = b.th.rd * feps;
+    rho[i] = pre[i] / (rho[i] * gam[i]);
+    pre[i] -= psv[i];
+  }
+  // :113-127 outflow walls hold T and p' constant into the ghosts
+  if (b.cfg.bc[0] == CANOE_BC_OUTFLOW)
+    for (int i = is - NG; i < is; ++i) {
+      rho[i] = rho[is];
+      pre[i] = pre[is];
+    }
+  if (b.cfg.bc[1] == CANOE_BC_OUTFLOW)
+    for (int i = ie + 1; i <= ie + NG; ++i) {
+      rho[i] = rho[ie];
+      pre[i] = pre[ie];
+    }
+}
+
+// Decomposition::RestoreFromTemperature for column (k, j)
+// (change_to_temperature.cpp:138-167): the pencil q back to rho and p, and
+// the face states wl / wr (nv x (nc1 + 1)) of faces lo..hi back to rho and p
+// with the hydrostatic face pressure added.
+void restore_from_temperature_pencil(Block &b, int k, int j, double *q, double *wl,
+                                     double *wr, int lo, int hi) {
+  const int nc1 = b.nc1, ipr = b.ipr;
+  const int is = b.is, ie = b.ie;
+  if (b.th.grav == 0.) return;
+  const double *psf = &b.psf[((size_t)k * b.nc2 + j) * (nc1 + 1)];
+  const double *psv = &b.psv[b.idx(0, k, j, 0)];
+  const double *gam = &b.gam[b.idx(0, k, j, 0)];
+  double *rho = &q[0], *pre = &q[ipr * nc1];
+  for (int i = is - NG; i <= ie + NG; ++i) {
+    pre[i] += psv[i];
+    rho[i] = pre[i] / (rho[i] * gam[i]);
+  }
+  double *lr = &wl[0], *lp = &wl[ipr * (nc1 + 1)];
+  double *rr = &wr[0], *rp = &wr[ipr * (nc1 + 1)];
+  for (int i = lo; i <= hi; ++i) {
+    rp[i] += psf[i];
+    if (rp[i] < 0.) rp[i] = psf[i];
+    double gamma = std::sqrt(gam[i] * gam[i - 1]);
+    rr[i] = rp[i] / (rr[i] * gamma);
+    lp[i] += psf[i];
+    if (lp[i] < 0.) lp[i] = psf[i];
+    lr[i] = lp[i] / (lr[i] * gamma);
+  }
+}
+
 static void flux_x1_pencil(Block &b, int k, int j, std::vector<double> &q,
                            std::vector<double> &wl, std::vector<double> &wr,
                            std::vector<double> &fx) {
   const int nc1 = b.nc1, nv = b.nv, ipr = b.ipr;
   const int is = b.is, ie = b.ie;
-  const double grav = b.th.grav;
   // pencil copy q(n, i)
   for (int n = 0; n < nv; ++n)
     for (int i = 0; i < nc1; ++i) q[n * nc1 + i] = b.w[b.idx(n, k, j, i)];
-  double *psf = &b.psf[((size_t)k * b.nc2 + j) * (nc1 + 1)];
-  double *psv = &b.psv[b.idx(0, k, j, 0)];
-  double *gam = &b.gam[b.idx(0, k, j, 0)];
-  double *rho = &q[0], *pre = &q[ipr * nc1];
-  if (grav != 0.) {
-    // change_to_temperature.cpp:57-64 isothermal extrapolation to the top
-    double RdTv = pre[ie] / rho[ie];
-    psf[ie + 1] = pre[ie] * std::exp(grav * b.dx1f[ie] / (2 * RdTv));
-    // :65 IntegrateDownwards (:30-38)
-    for (int i = ie; i >= is; --i) psf[i] = psf[i + 1] - grav * rho[i] * b.dx1f[i];
-    // :71-82 ghost psf, reflecting walls integrate with -grav
-    double gb = b.cfg.bc[0] == CANOE_BC_REFLECT ? -grav : grav;
-    for (int i = is - 1; i >= is - NG; --i) psf[i] = psf[i + 1] - gb * rho[i] * b.dx1f[i];
-    double gt = b.cfg.bc[1] == CANOE_BC_REFLECT ? -grav : grav;
-    for (int i = ie + 1; i <= ie + NG; ++i) psf[i + 1] = psf[i] + gt * rho[i] * b.dx1f[i];
-    // :89-111 per cell: log-mean psv, RovRd, rho -> T, p -> p'
-    for (int i = is - NG; i <= ie + NG; ++i) {
-      if (std::fabs(psf[i] - psf[i + 1]) < 1.E-6)
-        psv[i] = 0.5 * (psf[i] + psf[i + 1]);
-      else
-        psv[i] = (psf[i] - psf[i + 1]) / std::log(psf[i] / psf[i + 1]);
-      double feps = 1.;
-      for (int n = 1; n <= b.th.nvapor; ++n)
-        feps += q[n * nc1 + i] * b.th.inv_mu_ratio_m1[n - 1];
-      gam[i] = b.th.rd * feps;
-      rho[i] = pre[i] / (rho[i] * gam[i]);
-      pre[i] -= psv[i];
-    }
-    // :113-127 outflow walls hold T and p' constant into the ghosts
-    if (b.cfg.bc[0] == CANOE_BC_OUTFLOW)
-      for (int i = is - NG; i < is; ++i) {
-        rho[i] = rho[is];
-        pre[i] = pre[is];
-      }
-    if (b.cfg.bc[1] == CANOE_BC_OUTFLOW)
-      for (int i = ie + 1; i <= ie + NG; ++i) {
-        rho[i] = rho[ie];
-        pre[i] = pre[ie];
-      }
-  }
+  change_to_temperature_pencil(b, k, j, q.data());
   // reconstruct faces is..ie+1
   int lo = is, hi = ie + 1;
   for (int n = 0; n < nv; ++n) {
@@ -515,28 +553,13 @@ static void flux_x1_pencil(Block &b, int k, int j, std::vector<double> &q,
     else
       plm_line_nonuniform(qn, b.x1v.data(), b.x1f.data(), lo, hi, l, r);
   }
-  if (grav != 0.) {
-    // RestoreFromTemperature, change_to_temperature.cpp:150-164
-    for (int i = is - NG; i <= ie + NG; ++i) {
-      pre[i] += psv[i];
-      rho[i] = pre[i] / (rho[i] * gam[i]);
-    }
+  if (b.th.grav != 0.) {
+    restore_from_temperature_pencil(b, k, j, q.data(), wl.data(), wr.data(), lo, hi);
     if (b.fix_roundtrip)
       for (int i = 0; i < nc1; ++i) {
-        b.w[b.idx(0, k, j, i)] = rho[i];
-        b.w[b.idx(ipr, k, j, i)] = pre[i];
+        b.w[b.idx(0, k, j, i)] = q[i];
+        b.w[b.idx(ipr, k, j, i)] = q[ipr * nc1 + i];
       }
-    double *lr = &wl[0], *lp = &wl[ipr * (nc1 + 1)];
-    double *rr = &wr[0], *rp = &wr[ipr * (nc1 + 1)];
-    for (int i = lo; i <= hi; ++i) {
-      rp[i] += psf[i];
-      if (rp[i] < 0.) rp[i] = psf[i];
-      double gamma = std::sqrt(gam[i] * gam[i - 1]);
-      rr[i] = rp[i] / (rr[i] * gamma);
-      lp[i] += psf[i];
-      if (lp[i] < 0.) lp[i] = psf[i];
-      lr[i] = lp[i] / (lr[i] * gamma);
-    }
   }
   // Riemann solver on the packed faces lo..hi
   int nf = hi - lo + 1;

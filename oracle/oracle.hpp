@@ -99,6 +99,12 @@ void apply_bc(Block &b, std::vector<double> &w);
 void cons_to_prim_block(Block &b);
 void calculate_fluxes(Block &b);
 void calculate_fluxes_x1_only(Block &b);
+// the x1 hydrostatic decomposition of one column's pencil q (nv x nc1) and its
+// inverse on q and on face states wl / wr (nv x (nc1 + 1)) of faces lo..hi;
+// psf / psv / gamma_ of the column live in the block
+void change_to_temperature_pencil(Block &b, int k, int j, double *q);
+void restore_from_temperature_pencil(Block &b, int k, int j, double *q, double *wl,
+                                     double *wr, int lo, int hi);
 void add_flux_divergence(Block &b, double wght, std::vector<double> &du);
 void add_gravity_source(Block &b, double dt, std::vector<double> &du);
 void solve_implicit(Block &b, std::vector<double> &du, double dt);

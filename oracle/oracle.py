@@ -46,6 +46,10 @@ def load():
         ("oracle_periodic_block_solve", c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p,
                                                 c_void_p, c_void_p]),
         ("oracle_block_new_dt", c_double, [c_void_p]),
+        ("oracle_x1_change_to_temperature", c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                                    c_void_p, c_void_p]),
+        ("oracle_x1_restore_from_temperature", c_int, [c_void_p, c_int, c_int, c_void_p,
+                                                       c_void_p, c_void_p, c_int, c_int]),
         ("oracle_riemann", c_int, [c_int, POINTER(Thermo), c_int, c_void_p, c_void_p, c_void_p, c_int64]),
         ("oracle_cons_to_prim", c_int, [POINTER(Thermo), c_void_p, c_void_p, c_int64]),
         ("oracle_prim_to_cons", c_int, [POINTER(Thermo), c_void_p, c_void_p, c_int64]),
@@ -139,6 +143,28 @@ class OracleBlock:
 
     def new_dt(self):
         return self.lib.oracle_block_new_dt(self.h)
+
+    def x1_change_to_temperature(self, k, j):
+        """The x1 hydrostatic decomposition of column (k, j) of the current
+        primitive state: (q (nv, nc1) decomposed, psf, psv, gamma)."""
+        nv, nc1 = self.shape[0], self.shape[3]
+        q = np.zeros((nv, nc1))
+        psf = np.zeros(nc1 + 1)
+        psv = np.zeros(nc1)
+        gam = np.zeros(nc1)
+        self.lib.oracle_x1_change_to_temperature(self.h, k, j, q.ctypes.data, psf.ctypes.data,
+                                                 psv.ctypes.data, gam.ctypes.data)
+        return q, psf, psv, gam
+
+    def x1_restore_from_temperature(self, k, j, q, wl, wr, lo, hi):
+        """Its inverse with the column's arrays of the last call above:
+        returns (q, wl, wr) restored; wl / wr (nv, nc1 + 1), faces lo..hi."""
+        q = np.array(q, dtype=np.float64, order="C")
+        wl = np.array(wl, dtype=np.float64, order="C")
+        wr = np.array(wr, dtype=np.float64, order="C")
+        self.lib.oracle_x1_restore_from_temperature(self.h, k, j, q.ctypes.data, wl.ctypes.data,
+                                                    wr.ctypes.data, lo, hi)
+        return q, wl, wr
 
 
 def periodic_block_solve(a, b, c, rhs):
