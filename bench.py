@@ -170,27 +170,152 @@ LAUNCHES_PER_STEP = {"x1_pencil": 3, "flux_x2": 3, "flux_x3": 3, "unused": 0,
                      "satadj": 1, "cons_to_prim": 3, "dt": 1}
 
 
-def cpu_baseline(args, seconds=12.0, max_steps=20):
+def cpu_baseline(args, reps=5, seconds_per_rep=2.0, patch=32):
     """The oracle (C++ restatement, OpenMP over all host threads) on a bounded
-    sample of the workload: full 128-level columns on a 48 x 48 horizontal
-    patch, timed for about `seconds`."""
+    sample of the workload: full 128-level columns on a patch x patch
+    horizontal patch of the same configuration.  `reps` timed samples of at
+    least `seconds_per_rep` each (whole steps) with every host thread, and
+    `reps` single steps on one thread; each figure is the median of its
+    samples."""
     from oracle import oracle
     nthreads = oracle.set_threads(os.cpu_count() or 1)
-    p = make_problem(args, nx2=48, nx3=48)
+    p = make_problem(args, nx2=patch, nx3=patch)
     ob = oracle.OracleBlock(p)
     ncell = p.cfg.nx1 * p.cfg.nx2 * p.cfg.nx3
     ob.step(-1.0, 1)  # warm-up
-    t0 = time.perf_counter()
-    n = 0
-    while n < max_steps:
+    rates, steps = [], 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        n = 0
+        while n < 1 or time.perf_counter() - t0 < seconds_per_rep:
+            ob.step(-1.0, 1)
+            n += 1
+        rates.append(ncell * n / (time.perf_counter() - t0))
+        steps += n
+    oracle.set_threads(1)
+    single = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
         ob.step(-1.0, 1)
-        n += 1
-        if time.perf_counter() - t0 > seconds:
-            break
+        single.append(ncell / (time.perf_counter() - t0))
+    oracle.set_threads(nthreads)
+    return {"value": float(np.median(rates)), "unit": UNIT, "cores": nthreads, "kind": "port",
+            "single_thread": float(np.median(single)),
+            "samples": [float(r) for r in rates],
+            "sample": f"median of {reps} samples ({steps} steps in all) of a "
+                      f"{p.cfg.nx1}x{patch}x{patch} patch of the same configuration "
+                      f"({ncell} cells) on {nthreads} threads; single_thread: median of "
+                      f"{reps} single steps on 1 thread"}
+
+
+def c1_report(steps=2000, warmup=20, cpu_steps=200):
+    """C1: the 2-D dry rising bubble, 150 x 100, PLM + LMARS, no implicit
+    solve, FP64, every step with the device's CFL time step, stepped as a
+    replayed CUDA graph for the configuration's 2000 steps; beside it the
+    oracle on the host cores over `cpu_steps` steps of the same run."""
+    import torch
+    from canoe_b200 import MeshBlock, problems
+    from canoe_b200._abi import check
+    p = problems.bubble2d()
+    cells = p.cfg.nx1 * p.cfg.nx2 * p.cfg.nx3
+    stream = torch.cuda.Stream()
+    blk = MeshBlock(p, graph=True)
+    check(blk.lib.canoe_block_set_stream(blk.h, ctypes.c_void_p(stream.cuda_stream)))
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            blk.step()
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            blk.step()
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"config": "150 x 100 x 1, PLM + LMARS, FP64, no implicit solve, device CFL dt "
+                     "(0.8 split over the 2 directions) every step, graph replay",
+           "cells": cells, "steps": steps, "ms_per_step": ms / steps,
+           "value": cells * steps / (ms * 1e-3), "unit": UNIT,
+           "error_word": blk.error_word(),
+           "finite": bool(np.isfinite(blk.conserved()).all())}
+    blk.close()
+    from oracle import oracle
+    nthreads = oracle.set_threads(os.cpu_count() or 1)
+    ob = oracle.OracleBlock(problems.bubble2d())
+    ob.step(-1.0, 1)
+    t0 = time.perf_counter()
+    ob.step(-1.0, cpu_steps)
     el = time.perf_counter() - t0
-    return {"value": ncell * n / el, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": f"{n} steps of a 128x48x48 patch of the same configuration "
-                      f"({ncell} cells, {el:.1f} s wall)"}
+    out["cpu_oracle"] = {"value": cells * cpu_steps / el, "cores": nthreads,
+                         "sample": f"{cpu_steps} steps of the same run"}
+    return out
+
+
+def accuracy_report(args, net, nsteps):
+    """The north star's accuracy statement on the headline configuration:
+    the mixed + learned form and plain FP64 each advance C2 (full size) by
+    `nsteps` steps of the same fixed dt (the CFL step of the initial state)
+    from the same initial state; the relative L2 differences of potential
+    temperature and total water, the drift of total mass and total water of
+    each run, and the saturation adjustment's statistics over the run."""
+    import torch
+    from canoe_b200 import MeshBlock
+    from canoe_b200 import thermo as T_
+    from canoe_b200._abi import FP32_PERTURBATION, FP64
+    p = make_problem(args)
+    ny = p.ny
+    th = p.cfg.thermo
+    u0 = p.interior(p.u)
+    mass0, water0 = float(u0[:1 + ny].sum()), float(u0[1:1 + ny].sum())
+    del u0
+    res, dt0 = {}, None
+    for name, prec in (("fp64", FP64), ("mixed", FP32_PERTURBATION)):
+        p.cfg.precision = prec
+        b = MeshBlock(p, graph=True)
+        if name == "mixed":
+            b.set_mlp(net)
+        dt0 = dt0 or b.new_dt()
+        b.set_fixed_dt(dt0)
+        b.satadj_stats()
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            b.step()
+        b.synchronize()
+        el = time.perf_counter() - t0
+        s = b.satadj_stats()
+        u = p.interior(b.conserved())
+        w = p.interior(b.primitive())
+        cfl_end = b.new_dt()
+        vmax = float(np.abs(w[1 + ny:4 + ny]).max())
+        q = w[1:1 + ny]
+        T = w[4 + ny] / (w[0] * th.rd * T_.feps_of(th, q))
+        kap = (th.gammad - 1.0) / th.gammad
+        res[name] = {
+            "theta": T * (1.0e5 / w[4 + ny]) ** kap, "water": u[1:1 + ny].sum(axis=0),
+            "rec": {"wall_s": el, "error_word": b.error_word(),
+                    "mass_drift": float(u[:1 + ny].sum()) / mass0 - 1.0,
+                    "water_drift": float(u[1:1 + ny].sum()) / water0 - 1.0,
+                    "max_speed_end": vmax, "cfl_dt_end": cfl_end,
+                    "condensing_cells_end": int(((u[2:1 + ny] > 0).any(axis=0)).sum()),
+                    "satadj_evaluations_per_cell": float(s[1]) / max(1, int(s[0])),
+                    "satadj_fallback_rate": float(s[2]) / max(1, int(s[0])),
+                    "satadj_not_converged": int(s[3])}}
+        b.close()
+        del u, w
+        torch.cuda.empty_cache()
+
+    def rl2(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    return {"steps": nsteps, "dt": dt0, "bar": 1e-4,
+            "theta": rl2(res["mixed"]["theta"], res["fp64"]["theta"]),
+            "total_water": rl2(res["mixed"]["water"], res["fp64"]["water"]),
+            "fp64": res["fp64"]["rec"], "mixed": res["mixed"]["rec"],
+            "note": "relative L2 of the mixed + learned run against the plain FP64 run "
+                    "after the same steps; the FP64 GPU path matches the oracle to 1e-11 "
+                    "per step (tests/test_gpu_fullsize_parity.py); total water changes "
+                    "only through the implicit species correction of the reference "
+                    "(forward_backward.hpp:101-124)"}
 
 
 def c4_report(net, th, ncells=1 << 24, reps=3):
@@ -420,7 +545,7 @@ def c5_report(net, steps=5, warmup=2):
 def run_reference(args, rank):
     if rank != 0:
         return
-    cb = cpu_baseline(args, seconds=max(4.0, 2.0 * args.steps), max_steps=max(args.steps, 1))
+    cb = cpu_baseline(args, reps=max(3, min(args.steps, 5)))
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -463,17 +588,23 @@ def main():
     ap.add_argument("--no-c5", action="store_true")
     ap.add_argument("--implicit-flag", type=int, default=1, choices=[1, 9],
                     help="C2's implicit solve: 1 partial 3x3 (the headline), 9 full 5x5")
+    ap.add_argument("--no-c1", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 accuracy run on C2 (0: skip)")
     ap.add_argument("--no-5x5", action="store_true",
                     help="skip the full 5x5 implicit variant of C2")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
-                    help="c2: the headline line; c3 / c4 / c5: only that report, as one JSON line")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2: the headline line; c1 / c3 / c4 / c5: only that report, as one "
+                         "JSON line")
     ap.add_argument("--c4-cells", type=int, default=1 << 24,
                     help="cells of the C4 report (16.8 M by default)")
     args = ap.parse_args()
     if args.workload != "c2":
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        if args.workload == "c3":
+        if args.workload == "c1":
+            rep = c1_report()
+        elif args.workload == "c3":
             rep = c3_report(steps=args.steps, warmup=args.warmup)
         elif args.workload == "c4":
             from canoe_b200 import learned, thermo
@@ -639,22 +770,45 @@ def main():
                "h2d_bytes_per_step": nbytes / k, "d2h_bytes_per_step": nbytes / k + 8,
                "note": "state uploaded once and downloaded once per K-step run "
                        "(bytes amortised per step); dt read back every step"}
+        # K = 1 per call: the whole state up, one step, the whole state down,
+        # as a host that keeps its own arrays would call it at every step
+        k1 = max(3, min(k, 10))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k1):
+            check(lib.canoe_block_set_conserved(blk.h, ctypes.c_void_p(hu.data_ptr())))
+            check(lib.canoe_block_step(blk.h, -1.0))
+            check(lib.canoe_block_get_conserved(blk.h, ctypes.c_void_p(ho.data_ptr())))
+        el1 = time.perf_counter() - t0
+        e2e["per_call"] = {"value": world * ncell * k1 / el1, "unit": UNIT, "calls": k1,
+                           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                           "note": "every call uploads the state from pinned memory, steps "
+                                   "once and downloads the state"}
 
+    # the single-GPU reports run at N = 1 only (with N > 1 the other ranks
+    # would wait on rank 0 at the closing barrier)
+    solo = rank == 0 and world == 1
     cb = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if solo and not args.no_cpu_baseline:
         cb = cpu_baseline(args)
     c4 = None
     c3 = None
-    if rank == 0 and not args.no_c3:
+    if solo and not args.no_c3:
         c3 = c3_report()
+    c1 = None
+    if solo and not args.no_c1:
+        c1 = c1_report()
+    acc = None
+    if solo and args.accuracy_steps > 0:
+        acc = accuracy_report(args, net, args.accuracy_steps)
     c5 = None
-    if rank == 0 and not args.no_c5:
+    if solo and not args.no_c5:
         c5 = c5_report(net)
     f5 = None
-    if rank == 0 and not args.no_5x5:
+    if solo and not args.no_5x5:
         f5 = full5x5_report(args, net)
     fma = None
-    if rank == 0:
+    if solo:
         # non-tensor FMA peaks of this GPU (outside every timed region): the
         # denominator for the x1 pencil's FP64 arithmetic in profiles/
         p64, p32 = ctypes.c_double(0.), ctypes.c_double(0.)
@@ -663,7 +817,7 @@ def main():
         fma = {"fp64_tflops": p64.value, "fp32_tflops": p32.value,
                "how": "8 independent FMA chains per thread, 8 CTAs x 256 threads per SM, "
                       "CUDA events after a warm-up launch"}
-    if rank == 0 and not args.no_c4:
+    if solo and not args.no_c4:
         c4 = c4_report(net, p.cfg.thermo)
     if dist:
         dist.barrier()
@@ -679,6 +833,8 @@ def main():
             "other_variant": other, "speedup_mixed_vs_fp64":
                 (value / other["value"]) if args.precision == "mixed" else other["value"] / value,
             "l2_error_mixed_vs_fp64": l2, "saturation_adjustment": sat,
+            "accuracy_mixed_vs_fp64": acc,
+            "c1_dry_bubble": c1,
             "c4_learned_warm_start": c4,
             "c3_cubed_sphere_shell": c3,
             "c5_batched_blocks": c5,

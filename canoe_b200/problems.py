@@ -177,16 +177,18 @@ def moist_profile(th, z, Ts=300.0, Ttop=200.0, ps=1.0e5, rh=0.8, zmoist=10.0e3,
 
 def moist3d(nx1=128, nx2=256, nx3=256, x1max=16.0e3, x2max=64.0e3, x3max=64.0e3,
             seed=20240601, noise=0.1, noise_depth=1.0e3, implicit_flag=1,
-            recon=RECON_PPM, rsolver=RS_HLLC, satadj=1, cfl=0.4, th=None):
+            recon=RECON_PPM, rsolver=RS_HLLC, satadj=1, cfl=0.4, th=None, rh=0.8):
     """C2: 3-D moist convection LES initial state.  cfl as in bubble2d: the
     configuration's 0.8 split over the two horizontal directions (the
-    implicit x1 direction is limited by |v| only)."""
+    implicit x1 direction is limited by |v| only).  rh: relative humidity of
+    the moist layer (0.8 in the configuration; 1.0 makes the noise-cooled
+    cells condense at the first adjustment)."""
     th = th or T.earth_moist()
     ny = th.ny
     nv = 5 + ny
     x1f = np.linspace(0.0, x1max, nx1 + 1)
     z = 0.5 * (x1f[1:] + x1f[:-1])
-    temp, pres, qv = moist_profile(th, z)
+    temp, pres, qv = moist_profile(th, z, rh=rh)
     rng = np.random.Generator(np.random.PCG64(seed))
     dtn = rng.uniform(-noise, noise, size=(nx3, nx2, nx1))
     dtn *= (z < noise_depth)[None, None, :]
