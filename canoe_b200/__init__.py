@@ -10,3 +10,4 @@ from . import thermo, problems  # noqa: F401
 from .block import MeshBlock  # noqa: F401
 from .shell import Shell  # noqa: F401
 from .batch import Batch  # noqa: F401
+from .mesh import Mesh  # noqa: F401

@@ -11,7 +11,7 @@ MAX_NY = 8
 MAX_VAPOR = 4
 NGHOST = 3
 
-BC_REFLECT, BC_PERIODIC, BC_OUTFLOW, BC_EXO3 = 0, 1, 2, 3
+BC_REFLECT, BC_PERIODIC, BC_OUTFLOW, BC_EXO3, BC_BLOCK = 0, 1, 2, 3, 4
 RECON_PLM, RECON_PPM = 2, 3
 RS_LMARS, RS_HLLC = 0, 1
 FP64, FP32_PERTURBATION = 0, 1
@@ -109,6 +109,15 @@ SIGNATURES = [
     ("canoe_block_set_column_threads", c_int, [c_void_p, c_int]),
     ("canoe_selftest_bounded_wait", c_int, [c_int, c_int, c_void_p]),
     ("canoe_measure_fma_peak", c_int, [c_int, POINTER(c_double)]),
+    ("canoe_block_set_neighbor", c_int, [c_void_p, c_int, c_void_p]),
+    ("canoe_block_stage", c_int, [c_void_p, c_int, c_double]),
+    ("canoe_block_exchange_ghosts", c_int, [c_void_p]),
+    ("canoe_mesh_create", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    ("canoe_mesh_destroy", c_int, [c_void_p]),
+    ("canoe_mesh_use_graph", c_int, [c_void_p, c_int]),
+    ("canoe_mesh_step", c_int, [c_void_p, c_double]),
+    ("canoe_mesh_new_dt", c_int, [c_void_p, POINTER(c_double)]),
+    ("canoe_mesh_synchronize", c_int, [c_void_p]),
     ("canoe_batch_create", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     ("canoe_batch_destroy", c_int, [c_void_p]),
     ("canoe_batch_use_graph", c_int, [c_void_p, c_int]),

@@ -115,6 +115,21 @@ int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                   const MlpView *mlp = nullptr, double *guess_out = nullptr);
 MlpView mlp_view(const struct canoe_mlp *m);
 
+// ghost slabs copied between neighbouring blocks (exchange.cu): NV x nk x
+// nj rows of nc1 doubles; dst / src point at the first row's first cell,
+// variable and k strides in doubles for each side (j rows are nc1 apart)
+struct Slab {
+  double *dst;
+  const double *src;
+  int64_t dsv, dsk, ssv, ssk;
+  int nk, nj;
+};
+struct SlabSet {
+  Slab s[4];
+  int n, nv, nc1;
+};
+int launch_exchange(const SlabSet &ss, cudaStream_t st);
+
 // all checks a block configuration passes before a step runs on it (capi.cu);
 // 0 or a canoe_status with the message set
 int validate_block_config(const canoe_block_config_t &c);

@@ -4,6 +4,7 @@
 // runs CUDA kernels or returns an error.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -148,6 +149,10 @@ struct canoe_block {
   double fixed_dt = 0.;  // > 0: every step uses this dt instead of the CFL one
   canoe_mlp_t mlp = nullptr;  // learned warm start of the saturation adjustment
   size_t nvals = 0;
+  // block boundaries: the neighbour across each side and the ghost slabs of
+  // w that canoe_block_exchange_ghosts copies from the neighbours
+  canoe_block *nb[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  SlabSet slabs{};
 };
 
 // Every check a block configuration must pass before a step may run on it
@@ -175,6 +180,27 @@ int validate_block_config(const canoe_block_config_t &c) {
   if (c.precision != CANOE_FP64 && c.precision != CANOE_FP32_PERTURBATION) {
     set_error("precision must be CANOE_FP64 or CANOE_FP32_PERTURBATION");
     return CANOE_ERR_ARG;
+  }
+  for (int q = 0; q < 6; ++q) {
+    const int f = c.bc[q];
+    const bool phys = f == CANOE_BC_REFLECT || f == CANOE_BC_PERIODIC || f == CANOE_BC_OUTFLOW;
+    // x1 (the vertical) is never split between blocks: the hydrostatic scan
+    // and the implicit column solve stay in one block
+    if (!(phys || (q >= 2 && f == CANOE_BC_BLOCK))) {
+      set_error(q < 2 ? "x1 boundaries must be reflect, periodic or outflow"
+                      : "x2 / x3 boundaries must be reflect, periodic, outflow or block");
+      return CANOE_ERR_ARG;
+    }
+  }
+  if ((c.bc[2] == CANOE_BC_BLOCK || c.bc[3] == CANOE_BC_BLOCK) && c.nx2 > 1 &&
+      (c.implicit_flag & 2)) {
+    set_error("an implicit x2 solve across a block boundary is not provided");
+    return CANOE_ERR_UNSUPPORTED;
+  }
+  if ((c.bc[4] == CANOE_BC_BLOCK || c.bc[5] == CANOE_BC_BLOCK) && c.nx3 > 1 &&
+      (c.implicit_flag & 4)) {
+    set_error("an implicit x3 solve across a block boundary is not provided");
+    return CANOE_ERR_UNSUPPORTED;
   }
   if ((((c.implicit_flag & 2) && c.nx2 > 1) || ((c.implicit_flag & 4) && c.nx3 > 1)) &&
       c.thermo.ny > 0) {
@@ -241,68 +267,79 @@ static int line_solves(canoe_block *b, double *du, const double *dtp, const Stag
   return 0;
 }
 
-// one RK3 step, all launches on b->st; fixed_dt <= 0 uses the device dt
-static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullptr) {
+// one RK stage of block b on stream st (the per-stage task list up to
+// cons2prim with the physical boundaries); dtp: the step's device dt, acc:
+// the CFL accumulator fed at the last stage
+static int stage_launches(canoe_block *b, int s, double *dtp, unsigned long long *acc,
+                          cudaStream_t st, StepTimer *tm = nullptr) {
   const Geom &g = b->g;
+  const Stage &sg = kRK3[s];
   int rc;
 #define CB_MARK(c) \
-  if (tm && (rc = tm->mark(b->st, c))) return rc;
+  if (tm && (rc = tm->mark(st, c))) return rc;
   CB_MARK(-1);
+  if (g.f2 && (rc = launch_flux_x23(1, g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.precision,
+                                    b->d_w, b->d_du, dtp, sg.beta, nullptr, st)))
+    return rc;
+  CB_MARK(1);
+  if (g.f3 && (rc = launch_flux_x23(2, g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.precision,
+                                    b->d_w, b->d_du, dtp, sg.beta, nullptr, st)))
+    return rc;
+  CB_MARK(2);
+  if (!b->lines) {
+    if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                           b->cfg.precision, kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, dtp,
+                           sg, s, nullptr, st)))
+      return rc;
+  } else {
+    // du complete before the x3, x2, x1 solves (solve_implicit_3d.cpp:25-142)
+    if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                           b->cfg.precision, kColDivOnly, b->d_w, b->d_du, b->d_u, b->d_u1,
+                           dtp, sg, s, nullptr, st)))
+      return rc;
+    for (int dir = 2; dir >= 1; --dir) {
+      if (!line_solve_on(g, b->cfg.implicit_flag, dir)) continue;
+      const double *dxl = b->d_dxl + (dir == 2 ? g.nx2 + 2 * NG : 0);
+      if ((rc = launch_line_solve(dir, g, b->th, b->cfg.implicit_flag, b->d_w, b->d_du,
+                                  b->d_wt, b->d_dut, dxl, dtp, sg, st)))
+        return rc;
+    }
+    if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
+                           b->cfg.precision, kColSolveStep, b->d_w, b->d_du, b->d_u, b->d_u1,
+                           dtp, sg, s, nullptr, st)))
+      return rc;
+  }
+  CB_MARK(0);
+  if (s == 2 && b->cfg.satadj && b->th.ny > 0) {
+    canoe_satadj_opts_t o{1e-8, 30, b->mlp ? 2 : 0};
+    const int64_t nin = (int64_t)g.nx1 * g.nx2 * g.nx3;
+    MlpView mv;
+    if (b->mlp) mv = mlp_view(b->mlp);
+    if ((rc = launch_satadj(b->th, o, b->d_u, nin, g.sv, &g, nullptr, nullptr, nullptr,
+                            b->d_sat, st, b->mlp ? &mv : nullptr, nullptr)))
+      return rc;
+    CB_MARK(4);
+  }
+  if ((rc = launch_cons_to_prim(g, b->th, b->d_u, b->d_w, b->d_err, s == 2 ? acc : nullptr,
+                                b->cfg.cfl, b->cfg.implicit_flag, st)))
+    return rc;
+  CB_MARK(5);
+#undef CB_MARK
+  return 0;
+}
+
+// one RK3 step, all launches on b->st; fixed_dt <= 0 uses the device dt
+static int step_launches(canoe_block *b, double fixed_dt, StepTimer *tm = nullptr) {
+  int rc;
+  if (tm && (rc = tm->mark(b->st, -1))) return rc;
   if (fixed_dt > 0.) {
     // write the fixed dt; the accumulator reset is harmless here
     if ((rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, fixed_dt, b->st))) return rc;
   }
-  for (int s = 0; s < 3; ++s) {
-    const Stage &sg = kRK3[s];
-    CB_MARK(-1);
-    if (g.f2 && (rc = launch_flux_x23(1, g, b->th, b->cfg.recon, b->cfg.rsolver,
-                                      b->cfg.precision, b->d_w, b->d_du, b->d_dt, sg.beta,
-                                      nullptr, b->st)))
-      return rc;
-    CB_MARK(1);
-    if (g.f3 && (rc = launch_flux_x23(2, g, b->th, b->cfg.recon, b->cfg.rsolver,
-                                      b->cfg.precision, b->d_w, b->d_du, b->d_dt, sg.beta,
-                                      nullptr, b->st)))
-      return rc;
-    CB_MARK(2);
-    if (!b->lines) {
-      if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
-                             b->cfg.precision, kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, b->d_dt,
-                             sg, s, nullptr, b->st)))
-        return rc;
-    } else {
-      // du complete before the x3, x2, x1 solves (solve_implicit_3d.cpp:25-142)
-      if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
-                             b->cfg.precision, kColDivOnly, b->d_w, b->d_du, b->d_u, b->d_u1,
-                             b->d_dt, sg, s, nullptr, b->st)))
-        return rc;
-      if ((rc = line_solves(b, b->d_du, b->d_dt, sg))) return rc;
-      if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
-                             b->cfg.precision, kColSolveStep, b->d_w, b->d_du, b->d_u, b->d_u1,
-                             b->d_dt, sg, s, nullptr, b->st)))
-        return rc;
-    }
-    CB_MARK(0);
-    if (s == 2 && b->cfg.satadj && b->th.ny > 0) {
-      canoe_satadj_opts_t o{1e-8, 30, b->mlp ? 2 : 0};
-      const int64_t nin = (int64_t)g.nx1 * g.nx2 * g.nx3;
-      MlpView mv;
-      if (b->mlp) mv = mlp_view(b->mlp);
-      if ((rc = launch_satadj(b->th, o, b->d_u, nin, g.sv, &g, nullptr, nullptr, nullptr,
-                              b->d_sat, b->st, b->mlp ? &mv : nullptr, nullptr)))
-        return rc;
-      CB_MARK(4);
-    }
-    if ((rc = launch_cons_to_prim(g, b->th, b->d_u, b->d_w, b->d_err,
-                                  s == 2 ? b->d_dtacc : nullptr, b->cfg.cfl,
-                                  b->cfg.implicit_flag, b->st)))
-      return rc;
-    CB_MARK(5);
-  }
-  rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, b->fixed_dt, b->st);
-  if (rc) return rc;
-  CB_MARK(6);
-#undef CB_MARK
+  for (int s = 0; s < 3; ++s)
+    if ((rc = stage_launches(b, s, b->d_dt, b->d_dtacc, b->st, tm))) return rc;
+  if ((rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, b->fixed_dt, b->st))) return rc;
+  if (tm && (rc = tm->mark(b->st, 6))) return rc;
   return 0;
 }
 
@@ -574,8 +611,20 @@ int canoe_block_set_fixed_dt(canoe_block_t b, double dt) {
   return 0;
 }
 
+// a block with block boundaries needs its ghosts exchanged between stages
+static int needs_mesh(const canoe_block *b) {
+  for (int q = 2; q < 6; ++q)
+    if (b->cfg.bc[q] == CANOE_BC_BLOCK) {
+      set_error("a block with block boundaries steps through canoe_mesh_step, or per stage "
+                "with canoe_block_stage and canoe_block_exchange_ghosts");
+      return CANOE_ERR_UNSUPPORTED;
+    }
+  return 0;
+}
+
 int canoe_block_step(canoe_block_t b, double dt) {
   if (!b) return CANOE_ERR_ARG;
+  if (int rc = needs_mesh(b)) return rc;
   if (b->graph && !(dt > 0.)) {
     if (!b->gexec) {
       cudaGraph_t graph;
@@ -599,6 +648,7 @@ int canoe_block_step_profile(canoe_block_t b, double dt, float *ms, int nclass) 
     set_error("canoe_block_step_profile needs ms[7]");
     return CANOE_ERR_ARG;
   }
+  if (int rc = needs_mesh(b)) return rc;
   StepTimer tm;
   for (int q = 0; q < 64; ++q) CB_CUDA(cudaEventCreate(&tm.ev[q]));
   int rc = step_launches(b, dt, &tm);
@@ -685,6 +735,276 @@ int canoe_block_set_column_threads(canoe_block_t b, int threads) {
     cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;
   }
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// meshes of blocks on one GPU: ghost slabs copied between neighbours between
+// RK stages (Athena's SEND_HYD / RECV_HYD / SETB_HYD), the mesh-wide CFL dt
+
+namespace {
+
+// the ghost slab of b across side q (2 ix2, 3 ox2, 4 ix3, 5 ox3) and the
+// slab of nb's interior it is filled from; interior k (x2 sides) or j (x3
+// sides) only: the x2 flux pass reads j-ghosts at interior k and the x3 pass
+// k-ghosts at interior j, so the corner ghosts are never read
+Slab side_slab(const canoe_block *b, int q, const canoe_block *nb) {
+  const Geom &g = b->g, &h = nb->g;
+  Slab sl;
+  sl.dsv = g.sv;
+  sl.dsk = g.sk;
+  sl.ssv = h.sv;
+  sl.ssk = h.sk;
+  if (q == 2 || q == 3) {
+    sl.nk = g.nx3;
+    sl.nj = NG;
+    const int jd = q == 3 ? g.je + 1 : g.js - NG;  // first ghost row of b
+    const int js = q == 3 ? h.js : h.je - NG + 1;  // first interior row of nb
+    sl.dst = b->d_w + (int64_t)g.ks * g.sk + (int64_t)jd * g.nc1;
+    sl.src = nb->d_w + (int64_t)h.ks * h.sk + (int64_t)js * h.nc1;
+  } else {
+    sl.nk = NG;
+    sl.nj = g.nx2;
+    const int kd = q == 5 ? g.ke + 1 : g.ks - NG;
+    const int ks = q == 5 ? h.ks : h.ke - NG + 1;
+    sl.dst = b->d_w + (int64_t)kd * g.sk + (int64_t)g.js * g.nc1;
+    sl.src = nb->d_w + (int64_t)ks * h.sk + (int64_t)h.js * h.nc1;
+  }
+  return sl;
+}
+
+void rebuild_slabs(canoe_block *b) {
+  b->slabs.n = 0;
+  b->slabs.nv = b->g.nv;
+  b->slabs.nc1 = b->g.nc1;
+  for (int q = 2; q < 6; ++q)
+    if (b->nb[q]) b->slabs.s[b->slabs.n++] = side_slab(b, q, b->nb[q]);
+}
+
+}  // namespace
+
+struct canoe_mesh {
+  std::vector<canoe_block *> blocks;
+  cudaStream_t st = nullptr;
+  double *d_dt = nullptr;  // the mesh's step dt (2 doubles)
+  unsigned long long *d_acc = nullptr;  // mesh-wide CFL minimum
+  double fixed_dt = 0.;
+  bool graph = false;
+  cudaGraphExec_t gexec = nullptr;
+};
+
+static int mesh_free(canoe_mesh *m) {
+  if (!m) return 0;
+  if (m->st) cudaStreamSynchronize(m->st);
+  if (m->gexec) cudaGraphExecDestroy(m->gexec);
+  if (m->d_dt) cudaFree(m->d_dt);
+  if (m->d_acc) cudaFree(m->d_acc);
+  if (m->st) cudaStreamDestroy(m->st);
+  delete m;
+  return 0;
+}
+
+// one step of every block: per stage, every block's stage, then every
+// block's ghost exchange (main.cpp:119-121 over the task list of
+// ImplicitHydroTasks); fixed_dt <= 0 uses the mesh's device dt
+static int mesh_launches(canoe_mesh *m, double fixed_dt) {
+  int rc;
+  const canoe_block *b0 = m->blocks[0];
+  if (fixed_dt > 0. &&
+      (rc = launch_dt_finalize(m->d_dt, m->d_acc, b0->cfg.cfl, fixed_dt, m->st)))
+    return rc;
+  for (int s = 0; s < 3; ++s) {
+    for (canoe_block *b : m->blocks)
+      if ((rc = stage_launches(b, s, m->d_dt, m->d_acc, m->st))) return rc;
+    for (canoe_block *b : m->blocks)
+      if ((rc = launch_exchange(b->slabs, m->st))) return rc;
+  }
+  return launch_dt_finalize(m->d_dt, m->d_acc, b0->cfg.cfl, m->fixed_dt, m->st);
+}
+
+extern "C" {
+
+int canoe_block_set_neighbor(canoe_block_t b, int side, canoe_block_t nb) {
+  if (!b || !nb || side < 2 || side > 5) {
+    set_error("canoe_block_set_neighbor: null block or side outside 2..5");
+    return CANOE_ERR_ARG;
+  }
+  if (b->cfg.bc[side] != CANOE_BC_BLOCK) {
+    set_error("canoe_block_set_neighbor: the side's boundary flag is not CANOE_BC_BLOCK");
+    return CANOE_ERR_ARG;
+  }
+  const Geom &g = b->g, &h = nb->g;
+  const bool x2 = side < 4;
+  if ((x2 && !g.f2) || (!x2 && !g.f3)) {
+    set_error("canoe_block_set_neighbor: the block has no cells along that direction");
+    return CANOE_ERR_ARG;
+  }
+  if (g.nv != h.nv || g.nx1 != h.nx1 || g.nc1 != h.nc1 || b->cfg.precision != nb->cfg.precision ||
+      std::memcmp(&b->th, &nb->th, sizeof(canoe_thermo_t)) != 0) {
+    set_error("canoe_block_set_neighbor: neighbours share nx1, the thermodynamics and the "
+              "precision");
+    return CANOE_ERR_ARG;
+  }
+  std::vector<double> xa(g.nc1 + 1), xb(h.nc1 + 1);
+  CB_CUDA(cudaMemcpy(xa.data(), b->d_x1f, xa.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  CB_CUDA(cudaMemcpy(xb.data(), nb->d_x1f, xb.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  if (xa != xb) {
+    set_error("canoe_block_set_neighbor: neighbours share the x1 faces");
+    return CANOE_ERR_ARG;
+  }
+  // the shared face: x2 neighbours have the same nx3 (and f3), x3 ones the
+  // same nx2; the neighbour holds at least NGHOST cells across it
+  if (x2 ? (g.nx3 != h.nx3 || g.f3 != h.f3 || h.nx2 < NG || !h.f2)
+         : (g.nx2 != h.nx2 || h.nx3 < NG || !h.f3)) {
+    set_error("canoe_block_set_neighbor: the shared face differs or the neighbour is "
+              "thinner than NGHOST cells");
+    return CANOE_ERR_ARG;
+  }
+  b->nb[side] = nb;
+  rebuild_slabs(b);
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return 0;
+}
+
+int canoe_block_stage(canoe_block_t b, int stage, double dt) {
+  if (!b || stage < 0 || stage > 2) {
+    set_error("canoe_block_stage: null block or stage outside 0..2");
+    return CANOE_ERR_ARG;
+  }
+  int rc;
+  if (stage == 0 && dt > 0. &&
+      (rc = launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, dt, b->st)))
+    return rc;
+  if ((rc = stage_launches(b, stage, b->d_dt, b->d_dtacc, b->st))) return rc;
+  if (stage == 2)
+    return launch_dt_finalize(b->d_dt, b->d_dtacc, b->cfg.cfl, b->fixed_dt, b->st);
+  return 0;
+}
+
+int canoe_block_exchange_ghosts(canoe_block_t b) {
+  if (!b) return CANOE_ERR_ARG;
+  for (int q = 2; q < 6; ++q)
+    if (b->cfg.bc[q] == CANOE_BC_BLOCK && !b->nb[q]) {
+      set_error("canoe_block_exchange_ghosts: a block side has no neighbour");
+      return CANOE_ERR_ARG;
+    }
+  return launch_exchange(b->slabs, b->st);
+}
+
+int canoe_mesh_create(canoe_block_t *blocks, int n, canoe_mesh_t *out) {
+  if (!blocks || n < 1 || !out) {
+    set_error("canoe_mesh_create: null pointer or no blocks");
+    return CANOE_ERR_ARG;
+  }
+  *out = nullptr;
+  for (int q = 0; q < n; ++q) {
+    canoe_block *b = blocks[q];
+    if (!b) return CANOE_ERR_ARG;
+    for (int side = 2; side < 6; ++side) {
+      if (b->cfg.bc[side] != CANOE_BC_BLOCK) continue;
+      const canoe_block *nb = b->nb[side];
+      if (!nb || std::find(blocks, blocks + n, nb) == blocks + n) {
+        set_error("canoe_mesh_create: a block side names no neighbour of the mesh");
+        return CANOE_ERR_ARG;
+      }
+    }
+    if (b->cfg.cfl != blocks[0]->cfg.cfl || b->g.nc1 != blocks[0]->g.nc1) {
+      set_error("canoe_mesh_create: the blocks share the CFL number and nx1");
+      return CANOE_ERR_ARG;
+    }
+  }
+  canoe_mesh *m = new canoe_mesh();
+  m->blocks.assign(blocks, blocks + n);
+  cudaError_t e;
+  auto fail = [&](cudaError_t err, const char *what) {
+    int rc = cuda_status(err, what);
+    mesh_free(m);
+    return rc;
+  };
+  if ((e = cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking))) return fail(e, "stream");
+  if ((e = cudaMalloc(&m->d_dt, 2 * sizeof(double)))) return fail(e, "cudaMalloc dt");
+  if ((e = cudaMalloc(&m->d_acc, sizeof(unsigned long long)))) return fail(e, "cudaMalloc acc");
+  // the blocks' own work is done before the mesh takes over
+  for (canoe_block *b : m->blocks)
+    if ((e = cudaStreamSynchronize(b->st))) return fail(e, "block stream");
+  // the mesh-wide CFL dt of the current states and the FP32 path's
+  // reference pressure as the level mean over every block's columns
+  const int nc1 = blocks[0]->g.nc1;
+  std::vector<double> pref(nc1, 0.), pb(nc1);
+  double dtmin = 0., ncols = 0.;
+  for (canoe_block *b : m->blocks) {
+    double dtb = 0.;
+    if ((e = cudaMemcpy(&dtb, b->d_dt, sizeof(double), cudaMemcpyDeviceToHost)))
+      return fail(e, "copy dt");
+    dtmin = (dtmin == 0. || dtb < dtmin) ? dtb : dtmin;
+    if ((e = cudaMemcpy(pb.data(), b->d_pref, nc1 * sizeof(double), cudaMemcpyDeviceToHost)))
+      return fail(e, "copy pref");
+    const double c = (double)b->g.nx2 * b->g.nx3;
+    for (int i = 0; i < nc1; ++i) pref[i] += c * pb[i];
+    ncols += c;
+  }
+  for (int i = 0; i < nc1; ++i) pref[i] /= ncols;
+  for (canoe_block *b : m->blocks)
+    if ((e = cudaMemcpy(b->d_pref, pref.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice)))
+      return fail(e, "copy pref");
+  const double dt2[2] = {dtmin, 0.};
+  const unsigned long long inf = 0x7ff0000000000000ULL;
+  if ((e = cudaMemcpy(m->d_dt, dt2, sizeof(dt2), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  if ((e = cudaMemcpy(m->d_acc, &inf, sizeof(inf), cudaMemcpyHostToDevice))) return fail(e, "copy");
+  // the ghosts of block sides, from the states as they are
+  for (canoe_block *b : m->blocks)
+    if (int rc = launch_exchange(b->slabs, m->st)) {
+      mesh_free(m);
+      return rc;
+    }
+  if ((e = cudaStreamSynchronize(m->st))) return fail(e, "exchange");
+  *out = m;
+  return 0;
+}
+
+int canoe_mesh_destroy(canoe_mesh_t m) { return mesh_free(m); }
+
+int canoe_mesh_use_graph(canoe_mesh_t m, int on) {
+  if (!m) return CANOE_ERR_ARG;
+  m->graph = on != 0;
+  return 0;
+}
+
+int canoe_mesh_step(canoe_mesh_t m, double dt) {
+  if (!m) return CANOE_ERR_ARG;
+  if (m->graph && !(dt > 0.)) {
+    if (!m->gexec) {
+      cudaGraph_t graph;
+      CB_CUDA(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
+      int rc = mesh_launches(m, 0.);
+      cudaError_t e = cudaStreamEndCapture(m->st, &graph);
+      if (rc) return rc;
+      if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+      e = cudaGraphInstantiate(&m->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+    }
+    CB_CUDA(cudaGraphLaunch(m->gexec, m->st));
+    return 0;
+  }
+  return mesh_launches(m, dt);
+}
+
+int canoe_mesh_new_dt(canoe_mesh_t m, double *dt_out) {
+  if (!m || !dt_out) return CANOE_ERR_ARG;
+  CB_CUDA(cudaMemcpyAsync(dt_out, m->d_dt, sizeof(double), cudaMemcpyDeviceToHost, m->st));
+  CB_CUDA(cudaStreamSynchronize(m->st));
+  return 0;
+}
+
+int canoe_mesh_synchronize(canoe_mesh_t m) {
+  if (!m) return CANOE_ERR_ARG;
+  CB_CUDA(cudaStreamSynchronize(m->st));
   return 0;
 }
 

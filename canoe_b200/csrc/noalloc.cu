@@ -89,6 +89,11 @@ extern "C" int canoe_block_step_noalloc(const canoe_block_config_t *cfg, double 
   // the same checks as canoe_block_create: a configuration it refuses is
   // refused here too
   if (int rc = validate_block_config(*cfg)) return rc;
+  for (int q = 2; q < 6; ++q)
+    if (cfg->bc[q] == CANOE_BC_BLOCK) {
+      set_error("canoe_block_step_noalloc: block boundaries need a mesh (canoe_mesh_step)");
+      return CANOE_ERR_UNSUPPORTED;
+    }
   const canoe_thermo_t &th = cfg->thermo;
   const cudaStream_t st = (cudaStream_t)stream;
   Geom g{};

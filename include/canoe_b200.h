@@ -57,7 +57,10 @@ enum canoe_bc {
   CANOE_BC_REFLECT = 0,
   CANOE_BC_PERIODIC = 1,
   CANOE_BC_OUTFLOW = 2,
-  CANOE_BC_EXO3 = 3 /* cubed-sphere panel edge: ghosts filled by the exo3 exchange */
+  CANOE_BC_EXO3 = 3, /* cubed-sphere panel edge: ghosts filled by the exo3 exchange */
+  CANOE_BC_BLOCK = 4 /* x2 / x3 side shared with a neighbouring MeshBlock: ghosts
+                      * filled from the neighbour's interior (Athena's block
+                      * boundary, BoundaryFlag::block) */
 };
 
 /* reconstruction order (Athena `xorder`): 2 = PLM, 3 = PPM */
@@ -144,6 +147,7 @@ typedef struct canoe_shell_config {
 
 typedef struct canoe_shell *canoe_shell_t;
 typedef struct canoe_batch *canoe_batch_t;
+typedef struct canoe_mesh *canoe_mesh_t;
 
 /* ---------------- version / diagnostics ---------------- */
 const char *canoe_version(void);
@@ -366,6 +370,53 @@ int canoe_block_set_column_threads(canoe_block_t b, int threads);
  * (canoe_block_set_fixed_dt or its CFL step).  The reference steps its
  * MeshBlocks one after another in the task list (TaskList::
  * DoTaskListOneStage, called at main.cpp:119-121); no direct counterpart. */
+/* ---------------- meshes of MeshBlocks (block boundaries) ----------------
+ * Athena refreshes every block's ghost zones from its neighbours between RK
+ * stages with the boundary tasks SEND_HYD -> RECV_HYD -> SETB_HYD
+ * (patches/24.time_integrator.patch:17-19), run per stage by
+ * TaskList::DoTaskListOneStage over all blocks (main.cpp:119-121).  Here the
+ * blocks of a mesh stay resident on one GPU and a device copy fills the
+ * ghosts.  Blocks split the domain in x2 / x3 only (x1, the vertical, stays
+ * whole so that the hydrostatic scan and the implicit column solve stay in
+ * one block); neighbours share nx1, the x1 faces, the thermodynamics and the
+ * extent of the shared face. */
+
+/* Declare nb the neighbour of b across side (2 ix2, 3 ox2, 4 ix3, 5 ox3);
+ * b's bc[side] must be CANOE_BC_BLOCK.  A periodic domain is the mesh whose
+ * edge blocks name each other (Athena's periodic neighbour).
+ * BoundaryValues' neighbour list (bvals.hpp, NeighborBlock). */
+int canoe_block_set_neighbor(canoe_block_t b, int side, canoe_block_t nb);
+
+/* One RK stage (0, 1, 2) of one block on its stream: the per-stage task
+ * list of ImplicitHydroTasks (src/tasklist/implicit_hydro_tasks.cpp:45-313)
+ * up to cons2prim with the physical boundaries: CalculateFluxes ->
+ * IntegrateHydro -> AddSourceTerms -> ImplicitCorrection -> (stage 2)
+ * UpdateAllConserved -> ConservedToPrimitive.  dt > 0 at stage 0 sets the
+ * step's dt (the host's Mesh::dt); dt <= 0 keeps the device dt of the last
+ * completed step.  Stage 2 ends with the block's own CFL dt
+ * (canoe_block_new_dt), from which the host takes the mesh minimum
+ * (Mesh::NewTimeStep). */
+int canoe_block_stage(canoe_block_t b, int stage, double dt);
+
+/* SEND_HYD / RECV_HYD / SETB_HYD of block b as one device copy on b's
+ * stream: the NGHOST ghost layers of the primitive state on every
+ * CANOE_BC_BLOCK side are copied from the neighbour's interior.  The
+ * neighbours' stage must be complete (same stream, or ordered by the host). */
+int canoe_block_exchange_ghosts(canoe_block_t b);
+
+/* A mesh of blocks whose block sides name each other: canoe_mesh_step runs
+ * every RK stage of every block on the mesh's stream with the ghost
+ * exchange between stages and the mesh-wide CFL minimum (dt <= 0), as
+ * main.cpp:119-121 drives the task list.  Blocks must outlive the mesh.
+ * The FP32 flux path's reference pressure becomes the mesh-wide level mean
+ * of the blocks' states at creation. */
+int canoe_mesh_create(canoe_block_t *blocks, int n, canoe_mesh_t *out);
+int canoe_mesh_destroy(canoe_mesh_t m);
+int canoe_mesh_use_graph(canoe_mesh_t m, int on);
+int canoe_mesh_step(canoe_mesh_t m, double dt);
+int canoe_mesh_new_dt(canoe_mesh_t m, double *dt_out);
+int canoe_mesh_synchronize(canoe_mesh_t m);
+
 int canoe_batch_create(canoe_block_t *blocks, int n, canoe_batch_t *out);
 int canoe_batch_destroy(canoe_batch_t q);
 int canoe_batch_use_graph(canoe_batch_t q, int on);

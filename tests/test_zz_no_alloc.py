@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 FP32_PERTURBATION = 1
 CANOE_ERR_ARG = 1
-CANOE_ERR_UNSUPPORTED = 2
+CANOE_ERR_UNSUPPORTED = 5
 
 
 def _noalloc_two_steps(p, dt):
