@@ -112,6 +112,9 @@ SIGNATURES = [
     ("canoe_block_set_neighbor", c_int, [c_void_p, c_int, c_void_p]),
     ("canoe_block_stage", c_int, [c_void_p, c_int, c_double]),
     ("canoe_block_exchange_ghosts", c_int, [c_void_p]),
+    ("canoe_block_side_doubles", c_int, [c_void_p, c_int, POINTER(c_int64)]),
+    ("canoe_block_pack_side", c_int, [c_void_p, c_int, c_void_p]),
+    ("canoe_block_unpack_side", c_int, [c_void_p, c_int, c_void_p]),
     ("canoe_mesh_create", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     ("canoe_mesh_destroy", c_int, [c_void_p]),
     ("canoe_mesh_use_graph", c_int, [c_void_p, c_int]),

@@ -896,6 +896,73 @@ int canoe_block_exchange_ghosts(canoe_block_t b) {
   return launch_exchange(b->slabs, b->st);
 }
 
+static int side_ok(const canoe_block *b, int side) {
+  if (!b || side < 2 || side > 5 || (side < 4 && !b->g.f2) || (side >= 4 && !b->g.f3)) {
+    set_error("side must be 2..5 and the block must have cells along its direction");
+    return CANOE_ERR_ARG;
+  }
+  return 0;
+}
+
+int canoe_block_side_doubles(canoe_block_t b, int side, int64_t *n) {
+  if (int rc = side_ok(b, side)) return rc;
+  if (!n) return CANOE_ERR_ARG;
+  const Geom &g = b->g;
+  *n = (int64_t)g.nv * (side < 4 ? g.nx3 : g.nx2) * NG * g.nc1;
+  return 0;
+}
+
+// the layers of b next to `side` as a slab whose other end is a contiguous
+// buffer (rows in the order variable, k, j)
+static Slab buffer_slab(const canoe_block *b, int side, bool ghosts) {
+  const Geom &g = b->g;
+  Slab sl;
+  const bool x2 = side < 4, lo = (side & 1) == 0;
+  sl.nk = x2 ? g.nx3 : NG;
+  sl.nj = x2 ? NG : g.nx2;
+  int k0 = g.ks, j0 = g.js;
+  if (x2)
+    j0 = ghosts ? (lo ? g.js - NG : g.je + 1) : (lo ? g.js : g.je - NG + 1);
+  else
+    k0 = ghosts ? (lo ? g.ks - NG : g.ke + 1) : (lo ? g.ks : g.ke - NG + 1);
+  double *p = b->d_w + (int64_t)k0 * g.sk + (int64_t)j0 * g.nc1;
+  sl.dst = p;
+  sl.src = p;
+  sl.dsv = sl.ssv = g.sv;
+  sl.dsk = sl.ssk = g.sk;
+  return sl;
+}
+
+int canoe_block_pack_side(canoe_block_t b, int side, double *d_buf) {
+  if (int rc = side_ok(b, side)) return rc;
+  if (!d_buf) return CANOE_ERR_ARG;
+  Slab sl = buffer_slab(b, side, false);
+  sl.dst = d_buf;  // contiguous: k rows of nj x nc1, variables of nk rows
+  sl.dsk = (int64_t)sl.nj * b->g.nc1;
+  sl.dsv = (int64_t)sl.nk * sl.dsk;
+  SlabSet ss{};
+  ss.s[0] = sl;
+  ss.n = 1;
+  ss.nv = b->g.nv;
+  ss.nc1 = b->g.nc1;
+  return launch_exchange(ss, b->st);
+}
+
+int canoe_block_unpack_side(canoe_block_t b, int side, const double *d_buf) {
+  if (int rc = side_ok(b, side)) return rc;
+  if (!d_buf) return CANOE_ERR_ARG;
+  Slab sl = buffer_slab(b, side, true);
+  sl.src = d_buf;
+  sl.ssk = (int64_t)sl.nj * b->g.nc1;
+  sl.ssv = (int64_t)sl.nk * sl.ssk;
+  SlabSet ss{};
+  ss.s[0] = sl;
+  ss.n = 1;
+  ss.nv = b->g.nv;
+  ss.nc1 = b->g.nc1;
+  return launch_exchange(ss, b->st);
+}
+
 int canoe_mesh_create(canoe_block_t *blocks, int n, canoe_mesh_t *out) {
   if (!blocks || n < 1 || !out) {
     set_error("canoe_mesh_create: null pointer or no blocks");

@@ -188,6 +188,10 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     for (int q = q0; q < q1; ++q) mbar_wait(mbar + q, 0);
   };
 
+  // x1 spacing of this thread's first cell, read while the pencil rows are
+  // in flight (the hydrostatic scan's operands take it after the wait)
+  const double dx_first = g.dx1f[tid < nc1 ? tid : nc1 - 1];
+
   // P0: stage the pencil (and du)
   if (bulk) {
     if (tid == 0) {
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     if (grav != 0.)
       for (int i = tid; i < nc1; i += nth) {
         gam[i] = grav * wp[i];
-        psv[i] = g.dx1f[i];
+        psv[i] = i == tid ? dx_first : g.dx1f[i];
       }
     __syncthreads();
     // P2 for variable n over the cells is-1 .. ie+1, items t0, t0+dt, ...
@@ -581,6 +585,17 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     // c of the ghost row is-1 (periodic_forward_backward.hpp:67-72).
     const int nr = PER ? nx1 - 1 : nx1;
     double *zb = sm + L.z;  // PER: [nr][NN]
+    // 3x3, not periodic: cyclic reduction over levels s = 1 .. pcr/2 by the
+    // whole CTA, then parallel cyclic reduction (Hockney and Jesshope) of the
+    // at most 32 surviving rows in warp 0, one row per lane; pcr is the
+    // smallest power of two that leaves at most 32 rows.  Rows that a
+    // cyclic-reduction level eliminates are stored with a^-1, the rows that
+    // reach the parallel reduction with a itself.
+    int pcr = 1 << 30;
+    if constexpr (N == 3 && !PER) {
+      pcr = 1;
+      while (nr / pcr > 32) pcr *= 2;
+    }
     // face areas and the cell volume's reciprocal doubled, of row r
     auto row_geom = [&](int r, double &aL, double &aR, double &i2v) {
       const int i = is + r;
@@ -639,7 +654,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
             am.a[rr][qq] = a;
         }
         // N = 3: rows that the first level eliminates keep a^-1
-        if constexpr (N == 3) stm(row, ((r & 1) == 0 && 1 < nr) ? inv(am) : am);
+        if constexpr (N == 3) stm(row, ((r & 1) == 0 && 1 < nr && pcr > 1) ? inv(am) : am);
         put_rhs(r);
       }
       for (int r0 = 0; r0 < nx1; r0 += nth) {
@@ -772,7 +787,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
 #pragma unroll
         for (int e = 0; e < NN; ++e) cn.a[e / N][e % N] = 0.;
       }
-      const bool next_elim = (m & 1) == 0 && 4 * s - 1 < nr;
+      const bool next_elim = (m & 1) == 0 && 4 * s - 1 < nr && 2 * s < pcr;
       stm(row, next_elim ? inv(a) : a);
       stm(row + NN, bn);
       stm(row + 2 * NN, cn);
@@ -966,6 +981,81 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
         for (int m = seg; m < (nr + s) / (2 * s); m += nseg) back5(s, m);
         __syncthreads();
       }
+    } else if constexpr (N == 3 && !PER) {
+      for (int s = 1; s < pcr; s *= 2) {
+        for (int m = tid; m < nr / (2 * s); m += nth) level(s, m);
+        __syncthreads();
+      }
+      // the surviving rows r = pcr (q + 1) - 1, q < nq, form a block
+      // tridiagonal system of their own; each parallel-reduction level with
+      // stride d couples row q to q -/+ 2d, and after the last one every row
+      // is decoupled
+      if (warp == 0) {
+        const int nq = nr / pcr;
+        const bool act = lane < nq;
+        double *row = RP(act ? pcr * (lane + 1) - 1 : 0);
+        auto qrow = [&](int q) { return RP(pcr * (q + 1) - 1); };
+        for (int d = 1; d < nq; d *= 2) {
+          M<N> a;
+          if (act) {
+            a = ld(row);
+            stm(row, inv(a));  // neighbours read a^-1, b, c and rhs
+          }
+          __syncwarp();
+          M<N> an, bn, cn;
+          V<N> rn;
+          if (act) {
+            an = a;
+            rn = ldv(row + 3 * NN);
+            if (lane - d >= 0) {
+              const double *lo = qrow(lane - d);
+              M<N> al = mm(ld(row + NN), ld(lo));
+#pragma unroll
+              for (int e = 0; e < NN; ++e) al.a[e / N][e % N] = -al.a[e / N][e % N];
+              const M<N> t = mm(al, ld(lo + 2 * NN));
+              const V<N> tv = mv(al, ldv(lo + 3 * NN));
+#pragma unroll
+              for (int e = 0; e < NN; ++e) an.a[e / N][e % N] += t.a[e / N][e % N];
+#pragma unroll
+              for (int e = 0; e < N; ++e) rn.a[e] += tv.a[e];
+              bn = mm(al, ld(lo + NN));
+            } else {
+#pragma unroll
+              for (int e = 0; e < NN; ++e) bn.a[e / N][e % N] = 0.;
+            }
+            if (lane + d < nq) {
+              const double *hi = qrow(lane + d);
+              M<N> ga = mm(ld(row + 2 * NN), ld(hi));
+#pragma unroll
+              for (int e = 0; e < NN; ++e) ga.a[e / N][e % N] = -ga.a[e / N][e % N];
+              const M<N> t = mm(ga, ld(hi + NN));
+              const V<N> tv = mv(ga, ldv(hi + 3 * NN));
+#pragma unroll
+              for (int e = 0; e < NN; ++e) an.a[e / N][e % N] += t.a[e / N][e % N];
+#pragma unroll
+              for (int e = 0; e < N; ++e) rn.a[e] += tv.a[e];
+              cn = mm(ga, ld(hi + 2 * NN));
+            } else {
+#pragma unroll
+              for (int e = 0; e < NN; ++e) cn.a[e / N][e % N] = 0.;
+            }
+          }
+          __syncwarp();  // every lane has read its neighbours' rows
+          if (act) {
+            stm(row, an);
+            stm(row + NN, bn);
+            stm(row + 2 * NN, cn);
+            stv(row + 3 * NN, rn);
+          }
+          __syncwarp();
+        }
+        if (act) stv(row + 3 * NN, mv(inv(ld(row)), ldv(row + 3 * NN)));
+      }
+      __syncthreads();
+      for (int s = pcr / 2; s >= 1; s /= 2) {
+        for (int m = tid; m < (nr + s) / (2 * s); m += nth) back(s, m);
+        __syncthreads();
+      }
     } else {
       int stop = 1;  // first s with 2 s - 1 >= nr
       while (2 * stop - 1 < nr) stop *= 2;
@@ -1088,25 +1178,33 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
     }
   }
 
-  // P7b: write back
+  // P7b: write back.  A cell's NV values of u (and u1) are all loaded before
+  // any store, so that the loads are in flight together (stores to u could
+  // otherwise alias the next variable's load as far as the compiler knows)
   if constexpr (!UPDATE) {
     for (int n = 0; n < NV; ++n)
       for (int i = is + tid; i <= ie; i += nth) du[n * g.sv + base + i] = dc[n * nc1 + i];
   } else {
-    for (int n = 0; n < NV; ++n)
-      for (int i = is + tid; i <= ie; i += nth) {
-        const int64_t x = n * g.sv + base + i;
-        const double uo = u[x];
-        double ur;
-        if (stage == 0) {
-          u1[x] = uo;
-          ur = uo;
-        } else {
-          ur = u1[x];
+    for (int i = is + tid; i <= ie; i += nth) {
+      double uo[NV], ur[NV];
+#pragma unroll
+      for (int n = 0; n < NV; ++n) uo[n] = u[n * g.sv + base + i];
+      if (stage != 0) {
+#pragma unroll
+        for (int n = 0; n < NV; ++n) ur[n] = u1[n * g.sv + base + i];
+      } else {
+#pragma unroll
+        for (int n = 0; n < NV; ++n) {
+          ur[n] = uo[n];
+          u1[n * g.sv + base + i] = uo[n];
         }
-        const double t = st.g1 * uo + st.g2 * ur;
-        u[x] = t + dc[n * nc1 + i];
       }
+#pragma unroll
+      for (int n = 0; n < NV; ++n) {
+        const double t = st.g1 * uo[n] + st.g2 * ur[n];
+        u[n * g.sv + base + i] = t + dc[n * nc1 + i];
+      }
+    }
   }
 }
 

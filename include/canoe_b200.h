@@ -404,6 +404,20 @@ int canoe_block_stage(canoe_block_t b, int stage, double dt);
  * neighbours' stage must be complete (same stream, or ordered by the host). */
 int canoe_block_exchange_ghosts(canoe_block_t b);
 
+/* The ghost exchange across GPUs, for blocks whose neighbour lives on
+ * another device (each rank a process, one GPU each, the transfer by NCCL
+ * or peer copies): pack copies the NGHOST interior layers of b next to
+ * `side` -- what the neighbour across `side` needs -- into the contiguous
+ * device buffer d_buf; unpack writes a buffer received from the neighbour
+ * across `side` into b's ghost layers on that side.  Both run on b's
+ * stream.  Buffers hold NV x nx3 x NGHOST x nc1 doubles for an x2 side and
+ * NV x NGHOST x nx2 x nc1 for an x3 side (canoe_block_side_doubles).
+ * The MPI send / receive of Athena's BoundaryVariable (bvals_cc.cpp, with
+ * the cubed-sphere hook of patches/33.bvals_cc_cpp.patch:21). */
+int canoe_block_side_doubles(canoe_block_t b, int side, int64_t *n);
+int canoe_block_pack_side(canoe_block_t b, int side, double *d_buf);
+int canoe_block_unpack_side(canoe_block_t b, int side, const double *d_buf);
+
 /* A mesh of blocks whose block sides name each other: canoe_mesh_step runs
  * every RK stage of every block on the mesh's stream with the ghost
  * exchange between stages and the mesh-wide CFL minimum (dt <= 0), as
