@@ -186,81 +186,89 @@ __device__ __forceinline__ constexpr int sel(int r) {
   return N == 5 ? r : (r == 2 ? 4 : r);
 }
 
-// FluxJacobian (flux_decomposition.hpp:102-120), reduced to N x N
-template <int N, int NY>
-__device__ __forceinline__ void jacobian(M<N> &d, double gm1, const double *w) {
+// FluxJacobian (flux_decomposition.hpp:102-120), reduced to N x N, evaluated
+// in T (double; float for the FP32 flux path, whose implicit blocks are
+// formed from FP32 coefficients and eliminated in FP64)
+template <int N, int NY, typename T = double>
+__device__ __forceinline__ void jacobian(M<N> &d, double gm1_, const double *w) {
   using S = Slots<NY>;
-  double v1 = w[S::IVX], v2 = w[S::IVY], v3 = w[S::IVZ];
-  double rho = w[0], pres = w[S::IPR];
-  double s2 = v1 * v1 + v2 * v2 + v3 * v3;
-  double c1 = ((gm1 - 1) * s2 / 2 - (gm1 + 1) / gm1 * pres / rho) * v1;
-  double c2 = (gm1 + 1) / gm1 * pres / rho + s2 / 2 - gm1 * v1 * v1;
-  const double f[5][5] = {{0, 1., 0., 0., 0.},
-                          {gm1 * s2 / 2 - v1 * v1, (2. - gm1) * v1, -gm1 * v2, -gm1 * v3, gm1},
-                          {-v1 * v2, v2, v1, 0., 0.},
-                          {-v1 * v3, v3, 0., v1, 0.},
-                          {c1, c2, -gm1 * v2 * v1, -gm1 * v3 * v1, (gm1 + 1) * v1}};
+  const T gm1 = T(gm1_);
+  T v1 = T(w[S::IVX]), v2 = T(w[S::IVY]), v3 = T(w[S::IVZ]);
+  T rho = T(w[0]), pres = T(w[S::IPR]);
+  T s2 = v1 * v1 + v2 * v2 + v3 * v3;
+  T c1 = ((gm1 - T(1)) * s2 / T(2) - (gm1 + T(1)) / gm1 * pres / rho) * v1;
+  T c2 = (gm1 + T(1)) / gm1 * pres / rho + s2 / T(2) - gm1 * v1 * v1;
+  const T f[5][5] = {{T(0), T(1), T(0), T(0), T(0)},
+                     {gm1 * s2 / T(2) - v1 * v1, (T(2) - gm1) * v1, -gm1 * v2, -gm1 * v3, gm1},
+                     {-v1 * v2, v2, v1, T(0), T(0)},
+                     {-v1 * v3, v3, T(0), v1, T(0)},
+                     {c1, c2, -gm1 * v2 * v1, -gm1 * v3 * v1, (gm1 + T(1)) * v1}};
 #pragma unroll
   for (int r = 0; r < N; ++r)
 #pragma unroll
-    for (int c = 0; c < N; ++c) d.a[r][c] = f[sel<N>(r)][sel<N>(c)];
+    for (int c = 0; c < N; ++c) d.a[r][c] = double(f[sel<N>(r)][sel<N>(c)]);
 }
 
 // |A| = R |Lambda| R^-1 at the face between cells with primitive states wl,
 // wr: RoeAverage (:34-67), SoundSpeed, Eigenvalue (:70-75), Eigenvector
-// (:78-99); only the N x N reduced block is formed.
-template <int N, int NY>
+// (:78-99); only the N x N reduced block is formed, in T as jacobian.
+template <int N, int NY, typename T = double>
 __device__ __forceinline__ void abs_jacobian(M<N> &A, const canoe_thermo_t &th,
-                                             double gm1, const double *wl,
-                                             const double *wr) {
+                                             double gm1_, const double *wl_,
+                                             const double *wr_) {
   using S = Slots<NY>;
-  double prim[S::NV];
-  double sqrtdl = sqrt(wl[0]);
-  double sqrtdr = sqrt(wr[0]);
-  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  const T gm1 = T(gm1_);
+  T wl[S::NV], wr[S::NV], prim[S::NV];
+#pragma unroll
+  for (int n = 0; n < S::NV; ++n) {
+    wl[n] = T(wl_[n]);
+    wr[n] = T(wr_[n]);
+  }
+  T sqrtdl = sqrt(wl[0]);
+  T sqrtdr = sqrt(wr[0]);
+  T isdlpdr = T(1) / (sqrtdl + sqrtdr);
   prim[0] = sqrtdl * sqrtdr;
   prim[S::IVX] = (sqrtdl * wl[S::IVX] + sqrtdr * wr[S::IVX]) * isdlpdr;
   prim[S::IVY] = (sqrtdl * wl[S::IVY] + sqrtdr * wr[S::IVY]) * isdlpdr;
   prim[S::IVZ] = (sqrtdl * wl[S::IVZ] + sqrtdr * wr[S::IVZ]) * isdlpdr;
 #pragma unroll
   for (int n = 1; n <= NY; ++n) prim[n] = (sqrtdl * wl[n] + sqrtdr * wr[n]) * isdlpdr;
-  double el = wl[S::IPR] / gm1 + 0.5 * wl[0] *
-              (wl[S::IVX] * wl[S::IVX] + wl[S::IVY] * wl[S::IVY] + wl[S::IVZ] * wl[S::IVZ]);
-  double er = wr[S::IPR] / gm1 + 0.5 * wr[0] *
-              (wr[S::IVX] * wr[S::IVX] + wr[S::IVY] * wr[S::IVY] + wr[S::IVZ] * wr[S::IVZ]);
-  double hbar = ((el + wl[S::IPR]) / sqrtdl + (er + wr[S::IPR]) / sqrtdr) * isdlpdr;
-  prim[S::IPR] = (hbar - 0.5 * (prim[S::IVX] * prim[S::IVX] + prim[S::IVY] * prim[S::IVY] +
-                                prim[S::IVZ] * prim[S::IVZ])) *
-                 gm1 / (gm1 + 1.) * prim[0];
-  double cs = sound_speed<double, NY>(th, prim);
-  double r = prim[0], u = prim[S::IVX], v = prim[S::IVY], w = prim[S::IVZ],
-         p = prim[S::IPR];
-  double ke = 0.5 * (u * u + v * v + w * w);
-  double hp = (gm1 + 1.) / gm1 * p / r;
-  double h = hp + ke;
-  const double ihp = 1. / hp, i2hp = 0.5 * ihp, i2chp = i2hp / cs;
-  const double R[5][5] = {{1., 1., 1., 0., 0.},
-                          {u - cs, u, u + cs, 0., 0.},
-                          {v, v, v, 1., 0.},
-                          {w, w, w, 0., 1.},
-                          {h - u * cs, ke, h + u * cs, v, w}};
+  T el = wl[S::IPR] / gm1 + T(0.5) * wl[0] *
+         (wl[S::IVX] * wl[S::IVX] + wl[S::IVY] * wl[S::IVY] + wl[S::IVZ] * wl[S::IVZ]);
+  T er = wr[S::IPR] / gm1 + T(0.5) * wr[0] *
+         (wr[S::IVX] * wr[S::IVX] + wr[S::IVY] * wr[S::IVY] + wr[S::IVZ] * wr[S::IVZ]);
+  T hbar = ((el + wl[S::IPR]) / sqrtdl + (er + wr[S::IPR]) / sqrtdr) * isdlpdr;
+  prim[S::IPR] = (hbar - T(0.5) * (prim[S::IVX] * prim[S::IVX] + prim[S::IVY] * prim[S::IVY] +
+                                   prim[S::IVZ] * prim[S::IVZ])) *
+                 gm1 / (gm1 + T(1)) * prim[0];
+  T cs = sound_speed<T, NY>(th, prim);
+  T r = prim[0], u = prim[S::IVX], v = prim[S::IVY], w = prim[S::IVZ], p = prim[S::IPR];
+  T ke = T(0.5) * (u * u + v * v + w * w);
+  T hp = (gm1 + T(1)) / gm1 * p / r;
+  T h = hp + ke;
+  const T ihp = T(1) / hp, i2hp = T(0.5) * ihp, i2chp = i2hp / cs;
+  const T R[5][5] = {{T(1), T(1), T(1), T(0), T(0)},
+                     {u - cs, u, u + cs, T(0), T(0)},
+                     {v, v, v, T(1), T(0)},
+                     {w, w, w, T(0), T(1)},
+                     {h - u * cs, ke, h + u * cs, v, w}};
   // R^-1 of Eigenvector (:94-98) with the divisions by hp, 2 hp and
   // 2 cs hp taken as reciprocals
-  const double Ri[5][5] = {
+  const T Ri[5][5] = {
       {(cs * ke + u * hp) * i2chp, (-hp - cs * u) * i2chp, -v * i2hp, -w * i2hp, i2hp},
       {(hp - ke) * ihp, u * ihp, v * ihp, w * ihp, -ihp},
       {(cs * ke - u * hp) * i2chp, (hp - cs * u) * i2chp, -v * i2hp, -w * i2hp, i2hp},
-      {-v, 0., 1., 0., 0.},
-      {-w, 0., 0., 1., 0.}};
-  const double lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
+      {-v, T(0), T(1), T(0), T(0)},
+      {-w, T(0), T(0), T(1), T(0)}};
+  const T lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
 #pragma unroll
   for (int a = 0; a < N; ++a)
 #pragma unroll
     for (int b = 0; b < N; ++b) {
-      double s = 0.;
+      T s = T(0);
 #pragma unroll
       for (int k = 0; k < 5; ++k) s += (R[sel<N>(a)][k] * lam[k]) * Ri[k][sel<N>(b)];
-      A.a[a][b] = s;
+      A.a[a][b] = double(s);
     }
 }
 

@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
         wl[S::IVZ] *= psin;
       }
       M<N> J;
-      jacobian<N, NY>(J, gm1, wl);
+      jacobian<N, NY, R>(J, gm1, wl);
 #pragma unroll
       for (int e = 0; e < NN; ++e) pJ(t)[e] = J.a[e / N][e % N];
       if (t <= nx1) {
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
           wr[S::IVZ] *= psin;
         }
         M<N> A;
-        abs_jacobian<N, NY>(A, th, gm1, wl, wr);
+        abs_jacobian<N, NY, R>(A, th, gm1, wl, wr);
 #pragma unroll
         for (int e = 0; e < NN; ++e) pA(t)[e] = A.a[e / N][e % N];
       }
