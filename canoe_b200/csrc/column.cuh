@@ -367,9 +367,9 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       for (int t = tid; t < NV * ncell; t += nth) recon(t / ncell, is - 1 + t % ncell);
     }
     __syncthreads();
-    // P3 (F aliases q, which nobody reads after P2)
-    for (int f = is + tid; f <= ie + 1; f += nth) {
-      R wl[NV], wr[NV], fx[NV];
+    // P3 (F aliases q, which nobody reads after P2).  prep: the face states
+    // restored from the decomposition; solve: the Riemann flux; emit: F
+    auto prep = [&](int f, R *wl, R *wr) -> double {
 #pragma unroll
       for (int n = 0; n < NV; ++n) {
         wl[n] = WR[n * nc1 + f - 1];
@@ -398,6 +398,9 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
           wl[0] = pl / (wl[0] * gamma);
         }
       }
+      return pf;
+    };
+    auto solve = [&](R *wl, R *wr, double pf, R *fx) {
       if constexpr (GEO) {
         if constexpr (PERT)
           hllc_pert<R, NY, 0, true>(th, wl, wr, R(pf), fx, R(tab(kTabCosC, k, j)));
@@ -412,6 +415,8 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       } else {
         riemann<R, NY, RS, 0>(th, wl, wr, fx);
       }
+    };
+    auto emit = [&](int f, const R *fx, double pf) {
 #pragma unroll
       for (int n = 0; n < NV; ++n) F[n * (nx1 + 1) + (f - is)] = fx[n];
       if constexpr (MODE == kColFluxOnly) {
@@ -422,6 +427,12 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
           fout[(((int64_t)n * g.nc3 + k) * g.nc2 + j) * (nc1 + 1) + f] = v;
         }
       }
+    };
+    for (int f = is + tid; f <= ie + 1; f += nth) {
+      R wl[NV], wr[NV], fx[NV];
+      const double pf = prep(f, wl, wr);
+      solve(wl, wr, pf, fx);
+      emit(f, fx, pf);
     }
     if (bulk && load_du) {
       if (!__syncthreads_and(mbar_wait(mbar + 1, 0))) {
@@ -528,30 +539,29 @@ __global__ void __launch_bounds__(ColPlan<N, PER, GEO>::threads, ColPlan<N, PER,
       psin = tab(kTabSinC, k, j);
     }
     // P5a: |A| at face t (between cells is-1+t and is+t) and J of cell is-1+t
-    for (int t = tid; t < nx1 + 2; t += nth) {
-      const int ic = is - 1 + t;
-      double wl[NV], wr[NV];
+    auto cell_state = [&](int ic, double *v) {
 #pragma unroll
-      for (int n = 0; n < NV; ++n) wl[n] = wp[n * nc1 + ic];
+      for (int n = 0; n < NV; ++n) v[n] = wp[n * nc1 + ic];
       if constexpr (GEO) {
-        wl[S::IVY] += wl[S::IVZ] * pcos;
-        wl[S::IVZ] *= psin;
+        v[S::IVY] += v[S::IVZ] * pcos;
+        v[S::IVZ] *= psin;
       }
+    };
+    auto put_m = [&](double *p, const M<N> &m) {
+#pragma unroll
+      for (int e = 0; e < NN; ++e) p[e] = m.a[e / N][e % N];
+    };
+    for (int t = tid; t < nx1 + 2; t += nth) {
+      double wl[NV], wr[NV];
+      cell_state(is - 1 + t, wl);
       M<N> J;
       jacobian<N, NY, R>(J, gm1, wl);
-#pragma unroll
-      for (int e = 0; e < NN; ++e) pJ(t)[e] = J.a[e / N][e % N];
+      put_m(pJ(t), J);
       if (t <= nx1) {
-#pragma unroll
-        for (int n = 0; n < NV; ++n) wr[n] = wp[n * nc1 + ic + 1];
-        if constexpr (GEO) {
-          wr[S::IVY] += wr[S::IVZ] * pcos;
-          wr[S::IVZ] *= psin;
-        }
+        cell_state(is + t, wr);
         M<N> A;
         abs_jacobian<N, NY, R>(A, th, gm1, wl, wr);
-#pragma unroll
-        for (int e = 0; e < NN; ++e) pA(t)[e] = A.a[e / N][e % N];
+        put_m(pA(t), A);
       }
     }
     __syncthreads();
