@@ -10,9 +10,11 @@ advanced one step (canoe src/mesh_destroy.cpp:43-53).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank steps its own full block (weak scaling, no data
-collective: the path's blocks are independent between halo exchanges, which
-this build does not do across GPUs).  Rank 0 prints one JSON line.
+Under torchrun (N > 1) the ranks hold the N blocks of one periodic domain
+cut along x2, each block the configuration's full 128 x 256 x 256 (weak
+scaling): every RK stage exchanges the NGHOST ghost layers of the x2 block
+sides between ranks by NCCL point-to-point transfers
+(canoe_b200.distributed).  Rank 0 prints one JSON line.
 """
 import argparse
 import ctypes
@@ -143,12 +145,13 @@ def job_rates(ms_list, cells_per_rank, steps, dist=None, device="cuda"):
     return ms, [world * cells_per_rank * steps / (m * 1e-3) for m in ms]
 
 
-def make_problem(args, nx2=None, nx3=None):
+def make_problem(args, nx2=None, nx3=None, seed_offset=0):
     from canoe_b200 import problems
     return problems.moist3d(nx1=args.nx1, nx2=nx2 or args.nx2, nx3=nx3 or args.nx3,
                             x1max=16.0e3, x2max=64.0e3 * (nx2 or args.nx2) / 256,
                             x3max=64.0e3 * (nx3 or args.nx3) / 256,
-                            implicit_flag=getattr(args, "implicit_flag", 1))
+                            implicit_flag=getattr(args, "implicit_flag", 1),
+                            seed=20240601 + seed_offset)
 
 
 def algorithmic_bytes(nv, ny, ncell):
@@ -433,6 +436,10 @@ def full5x5_report(args, net, steps=5, warmup=2):
     FullCorrection of most of the reference's example inputs): mixed +
     learned against plain FP64, whole steps and the x1 pencil per launch."""
     import torch
+    if world > 1:
+        run_partitioned(args, dist, rank, world)
+        return
+
     from canoe_b200 import MeshBlock
     from canoe_b200._abi import FP32_PERTURBATION, FP64, check, load
     lib = load()
@@ -556,6 +563,75 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_partitioned(args, dist, rank, world):
+    """N > 1: the ranks' blocks tile one periodic domain along x2 (block q on
+    rank q, each the full configuration), stepped with the x2 ghost layers
+    exchanged by NCCL every RK stage; both precisions, the mixed one with the
+    learned warm start.  Timed on each rank with CUDA events on the stream
+    that carries the kernels and the transfers, the max over ranks."""
+    import torch
+    from canoe_b200 import distributed, learned
+    from canoe_b200._abi import BC_BLOCK, FP32_PERTURBATION, FP64
+    net = learned.default_net()
+    ncell = args.nx1 * args.nx2 * args.nx3
+    neighbors = [{2: (q - 1) % world, 3: (q + 1) % world} for q in range(world)]
+    order = [args.precision] + [k for k in ("fp64", "mixed") if k != args.precision]
+    results, dt0, clocks = {}, None, None
+    for name in order:
+        p = make_problem(args, seed_offset=rank)
+        p.cfg.precision = FP32_PERTURBATION if name == "mixed" else FP64
+        p.cfg.bc[2] = p.cfg.bc[3] = BC_BLOCK
+        dm = distributed.DistributedMesh({rank: p}, neighbors, list(range(world)),
+                                         distributed.GpuBackend(), dist)
+        if name == "mixed":
+            dm.blocks[rank].set_mlp(net)
+        dt0 = dt0 or dm.dt
+        stream = torch.cuda.current_stream()
+        sampler = ClockSampler(torch.cuda.current_device()) if name == args.precision else None
+        if sampler:
+            sampler.start()
+        for _ in range(args.warmup):
+            dm.step(dt0, update_dt=False)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.mark_begin()
+        e0.record(stream)
+        for _ in range(args.steps):
+            dm.step(dt0, update_dt=False)
+        e1.record(stream)
+        e1.synchronize()
+        if sampler:
+            sampler.mark_end()
+            clocks = sampler.stop()
+        results[name] = (e0.elapsed_time(e1), dm.blocks[rank].error_word())
+        dist.barrier()
+        dm.close()
+        torch.cuda.empty_cache()
+    (ms, ms_o), (value, value_o) = job_rates([results[order[0]][0], results[order[1]][0]],
+                                             ncell, args.steps, dist)
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank != 0:
+        return
+    cfg = config_dict(args)
+    cfg["parallelism"] = (f"{world} GPUs, one 128x256x256 block each, periodic domain cut "
+                          "along x2, NCCL halo exchange of 3 ghost layers every RK stage")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded C2 initial state per block)", "config": cfg,
+            "gpu_launches": args.steps * 27,  # 15 kernels of the stages, 12 packs / unpacks
+            "other_variant": {"variant": order[1], "value": value_o,
+                              "ms_per_step": ms_o / args.steps},
+            "roofline": None, "cpu_baseline": None, "e2e": None, "clocks": clocks,
+            "error_word": int(results[order[0]][1])}
+    print(json.dumps(line), flush=True)
+
+
 def config_dict(args):
     return {"workload": f"C2 3-D moist convection LES {args.nx1}x{args.nx2}x{args.nx3}, "
                         "PPM + HLLC, implicit X1 "
@@ -629,6 +705,10 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if world > 1:
+        run_partitioned(args, dist, rank, world)
+        return
 
     from canoe_b200 import MeshBlock
     from canoe_b200._abi import FP32_PERTURBATION, FP64, check, load

@@ -121,6 +121,17 @@ int oracle_block_step(void *h, double dt, int nsteps) {
 
 double oracle_block_new_dt(void *h) { return oracle::new_dt(*static_cast<Block *>(h)); }
 
+int oracle_block_stage(void *h, int stage, double dt) {
+  Block &b = *static_cast<Block *>(h);
+  try {
+    oracle::stage_step(b, dt, stage);
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  return 0;
+}
+
 // The x1 hydrostatic decomposition of column (k, j) of the block's primitive
 // state: q (nv x nc1) receives the decomposed pencil (T, p'), psf (nc1 + 1),
 // psv and gam (nc1) the column's hydrostatic arrays.

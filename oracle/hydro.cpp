@@ -384,6 +384,8 @@ void ppm_line(const double *q, int lo, int hi, double *ql, double *qr) {
 // ---------------------------------------------------------------------------
 // ghost cells (Athena reflecting / periodic / outflow conditions, restated)
 
+// A CANOE_BC_BLOCK side is left as it is: its ghosts come from the
+// neighbouring block (the exchange of the caller).
 void apply_bc(Block &b, std::vector<double> &w) {
   const int *bc = b.cfg.bc;
   // x1 over interior (j, k)
@@ -407,12 +409,15 @@ void apply_bc(Block &b, std::vector<double> &w) {
           for (int i = 0; i < b.nc1; ++i) {
             double s = (n == b.ivy) ? -1. : 1.;
             size_t lo = b.idx(n, k, b.js - g, i), hi = b.idx(n, k, b.je + g, i);
+            const double wlo = w[lo], whi = w[hi];
             if (bc[2] == CANOE_BC_REFLECT) w[lo] = s * w[b.idx(n, k, b.js + g - 1, i)];
             else if (bc[2] == CANOE_BC_PERIODIC) w[lo] = w[b.idx(n, k, b.je - g + 1, i)];
             else w[lo] = w[b.idx(n, k, b.js, i)];
             if (bc[3] == CANOE_BC_REFLECT) w[hi] = s * w[b.idx(n, k, b.je - g + 1, i)];
             else if (bc[3] == CANOE_BC_PERIODIC) w[hi] = w[b.idx(n, k, b.js + g - 1, i)];
             else w[hi] = w[b.idx(n, k, b.je, i)];
+            if (bc[2] == CANOE_BC_BLOCK) w[lo] = wlo;
+            if (bc[3] == CANOE_BC_BLOCK) w[hi] = whi;
           }
   if (b.f3)
     for (int n = 0; n < b.nv; ++n)
@@ -421,12 +426,15 @@ void apply_bc(Block &b, std::vector<double> &w) {
           for (int i = 0; i < b.nc1; ++i) {
             double s = (n == b.ivz) ? -1. : 1.;
             size_t lo = b.idx(n, b.ks - g, j, i), hi = b.idx(n, b.ke + g, j, i);
+            const double wlo = w[lo], whi = w[hi];
             if (bc[4] == CANOE_BC_REFLECT) w[lo] = s * w[b.idx(n, b.ks + g - 1, j, i)];
             else if (bc[4] == CANOE_BC_PERIODIC) w[lo] = w[b.idx(n, b.ke - g + 1, j, i)];
             else w[lo] = w[b.idx(n, b.ks, j, i)];
             if (bc[5] == CANOE_BC_REFLECT) w[hi] = s * w[b.idx(n, b.ke - g + 1, j, i)];
             else if (bc[5] == CANOE_BC_PERIODIC) w[hi] = w[b.idx(n, b.ks + g - 1, j, i)];
             else w[hi] = w[b.idx(n, b.ke, j, i)];
+            if (bc[4] == CANOE_BC_BLOCK) w[lo] = wlo;
+            if (bc[5] == CANOE_BC_BLOCK) w[hi] = whi;
           }
 }
 
@@ -747,12 +755,11 @@ double new_dt(const Block &b) {
 // 134-190): u = g1 u + g2 u1; du = -beta dt div F + sources; implicit
 // correction (:267-288); u += du; saturation adjustment at the last stage
 // (:290-313); then boundaries and cons2prim.
-void step(Block &b, double dt) {
+void stage_step(Block &b, double dt, int stage) {
   static const double g1[3] = {0., 0.25, 2. / 3.};
   static const double g2[3] = {1., 0.75, 1. / 3.};
   static const double be[3] = {1., 0.25, 2. / 3.};
-  size_t s = b.cells();
-  for (int stage = 0; stage < 3; ++stage) {
+  {
     calculate_fluxes(b);
 #pragma omp parallel for collapse(3) schedule(static)
     for (int n = 0; n < b.nv; ++n)
@@ -782,7 +789,10 @@ void step(Block &b, double dt) {
     }
     cons_to_prim_block(b);
   }
-  (void)s;
+}
+
+void step(Block &b, double dt) {
+  for (int stage = 0; stage < 3; ++stage) stage_step(b, dt, stage);
 }
 
 }  // namespace oracle

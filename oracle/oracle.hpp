@@ -115,6 +115,9 @@ int periodic_block_solve(int nb, int n, const double *a, const double *b, const 
                          const double *rhs, double *x);
 double new_dt(const Block &b);
 void step(Block &b, double dt);
+// one RK stage (0, 1, 2) of step(): fluxes, divergence, sources, implicit
+// correction, register update, saturation adjustment at stage 2, cons2prim
+void stage_step(Block &b, double dt, int stage);
 
 // cubed-sphere shell (exo3.cpp) ------------------------------------------------
 struct Shell {

@@ -46,6 +46,7 @@ def load():
         ("oracle_periodic_block_solve", c_int, [c_int, c_int, c_void_p, c_void_p, c_void_p,
                                                 c_void_p, c_void_p]),
         ("oracle_block_new_dt", c_double, [c_void_p]),
+        ("oracle_block_stage", c_int, [c_void_p, c_int, c_double]),
         ("oracle_x1_change_to_temperature", c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p,
                                                     c_void_p, c_void_p]),
         ("oracle_x1_restore_from_temperature", c_int, [c_void_p, c_int, c_int, c_void_p,
@@ -143,6 +144,11 @@ class OracleBlock:
 
     def new_dt(self):
         return self.lib.oracle_block_new_dt(self.h)
+
+    def stage(self, stage, dt):
+        """one RK stage of the oracle's step (ghosts of block sides untouched)"""
+        rc = self.lib.oracle_block_stage(self.h, stage, float(dt))
+        assert rc == 0, self.lib.oracle_last_error().decode()
 
     def x1_change_to_temperature(self, k, j):
         """The x1 hydrostatic decomposition of column (k, j) of the current

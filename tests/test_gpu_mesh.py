@@ -142,3 +142,30 @@ def test_block_sides_need_the_mesh():
         MeshBlock(r)
     b.close()
     other.close()
+
+
+def test_distributed_driver_on_one_gpu_reproduces_single_block():
+    """canoe_b200.distributed with every block on this GPU: the ghost slabs
+    travel through canoe_block_pack_side / canoe_block_unpack_side (the
+    buffers a multi-GPU run hands to NCCL) and the step equals the single
+    block's bit for bit."""
+    from canoe_b200 import distributed
+    p = perturb(_c2(), dv=0.5)
+    one = MeshBlock(p)
+    dm = distributed.DistributedMesh.from_domain(p, 2, 2)
+    assert dm.dt == one.new_dt()
+    for _ in range(3):
+        dt = dm.step()
+        one.step(dt)
+    from canoe_b200 import partition
+    got = partition.gather(dm_split(p, 2, 2), p.u.shape,
+                           [dm.conserved(q) for q in range(4)], p.cfg.nx2, p.cfg.nx3)
+    assert np.array_equal(p.interior(got), p.interior(one.conserved()))
+    assert dm.dt == one.new_dt()
+    dm.close()
+    one.close()
+
+
+def dm_split(p, nb2, nb3):
+    from canoe_b200 import partition
+    return partition.split(p, nb2, nb3)
