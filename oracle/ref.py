@@ -18,7 +18,7 @@ from canoe_b200._abi import Thermo
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 REF = os.environ.get("CANOE_REFERENCE", "/root/reference")
-UNITS = ("lmars", "hllc", "decomp")
+UNITS = ("lmars", "hllc", "decomp", "implicit")
 NHS = (5, 8)
 
 _libs = {}
@@ -59,6 +59,10 @@ def lib(unit, nh):
         L.ref_sound_speed.restype = c_int
         L.ref_sound_speed.argtypes = [POINTER(Thermo), c_double, c_double, c_void_p, c_void_p,
                                       c_int64]
+    elif unit == "implicit":
+        L.ref_implicit_correction.restype = c_int
+        L.ref_implicit_correction.argtypes = [POINTER(Thermo), c_double, c_double] + \
+            [c_int] * 10 + [c_void_p, c_double, c_double, c_void_p, c_void_p, c_double]
     else:
         L.ref_change_to_temperature.restype = c_int
         L.ref_change_to_temperature.argtypes = [POINTER(Thermo), c_double] + [c_int] * 5 + \
@@ -130,3 +134,19 @@ def restore_from_temperature(th, mu_d, is_, ie, dx1f, bc, psf, psv, gam, w, wl, 
                                              psv.ctypes.data, gam.ctypes.data, w.ctypes.data,
                                              wl.ctypes.data, wr.ctypes.data, k, j, il, iu))
     return w, wl, wr
+
+
+def implicit_correction(th, mu_d, cvd_R, full, w, du, dx1f, dx2, dx3, is_, ie, js, je, ks, ke,
+                        dt):
+    """The reference's ImplicitSolver (PartialCorrection, or FullCorrection
+    when full) over the interior columns of a Cartesian block: returns du
+    (NV, nc3, nc2, nc1) corrected, from the primitive state w."""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    du = np.array(du, dtype=np.float64, order="C")
+    nv, nc3, nc2, nc1 = w.shape
+    dx1f = np.ascontiguousarray(dx1f, dtype=np.float64)
+    L = lib("implicit", nv)
+    _check(L, L.ref_implicit_correction(ctypes.byref(th), mu_d, cvd_R, 1 if full else 0, nc3,
+                                        nc2, nc1, is_, ie, js, je, ks, ke, dx1f.ctypes.data,
+                                        dx2, dx3, w.ctypes.data, du.ctypes.data, dt))
+    return du

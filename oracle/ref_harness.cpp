@@ -13,6 +13,12 @@
 //   REF_UNIT_DECOMP   Decomposition::ChangeToTemperature and
 //                     RestoreFromTemperature of
 //                     src/snap/decomposition/change_to_temperature.cpp
+//   REF_UNIT_IMPLICIT ImplicitSolver::PartialCorrection and FullCorrection of
+//                     src/snap/implicit/{partial,full}_correction.cpp with
+//                     the ForwardSweep / BackwardSubstitution and the flux
+//                     decomposition of forward_backward.hpp and
+//                     flux_decomposition.hpp, and SoundSpeed of
+//                     src/snap/eos/ideal_moist_hydro.cpp
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -33,6 +39,9 @@
 #ifdef REF_UNIT_DECOMP
 #include <checks.hpp>
 #include <snap/decomposition/decomposition.hpp>
+#endif
+#ifdef REF_UNIT_IMPLICIT
+#include <snap/implicit/implicit_solver.hpp>
 #endif
 
 namespace {
@@ -77,7 +86,7 @@ struct RefBlock {
 
 }  // namespace
 
-#ifdef REF_UNIT_RIEMANN
+#if defined(REF_UNIT_RIEMANN) || defined(REF_UNIT_IMPLICIT)
 // EquationOfState's general-EOS hooks: declared by Athena++, reached only
 // when GENERAL_EOS is set (it is not in canoe's ideal-moist build).
 Real EquationOfState::EgasFromRhoP(Real, Real) {
@@ -86,6 +95,9 @@ Real EquationOfState::EgasFromRhoP(Real, Real) {
 Real EquationOfState::AsqFromRhoP(Real, Real) {
   throw std::runtime_error("general EOS is not part of this build");
 }
+#endif
+
+#ifdef REF_UNIT_RIEMANN
 
 extern "C" {
 
@@ -245,3 +257,80 @@ int ref_nhydro() { return NHYDRO; }
 
 }  // extern "C"
 #endif  // REF_UNIT_DECOMP
+
+#ifdef REF_UNIT_IMPLICIT
+// The members of ImplicitSolver that implicit_solver.cpp (input parsing, MPI
+// set-up, the direction switch) would define: one block, whole columns,
+// the x1 direction, reflecting ends (first and last block, not periodic).
+namespace {
+int gi_nc1 = 0, gi_nc2 = 0, gi_nc3 = 0;
+AthenaArray<Real> *g_du = nullptr;
+}  // namespace
+
+ImplicitSolver::ImplicitSolver(MeshBlock *pmb, ParameterInput *) : pmy_block_(pmb) {
+  implicit_flag_ = 1;
+  mydir_ = X1DIR;
+  has_top_neighbor = has_bot_neighbor = false;
+  first_block = last_block = true;
+  periodic_boundary = false;
+  pole_at_bot = pole_at_top = false;
+  buffer_ = nullptr;
+  du_.NewAthenaArray(NHYDRO, gi_nc3, gi_nc2, gi_nc1);
+  coefficients_.NewAthenaArray(gi_nc3, gi_nc2, gi_nc1, 100);
+  g_du = &du_;
+}
+ImplicitSolver::~ImplicitSolver() {}
+
+extern "C" {
+
+// SolveImplicit3D's x1 part (solve_implicit_3d.cpp:92-142) on a Cartesian
+// block: du (NHYDRO, nc3, nc2, nc1) is corrected in place column by column
+// by PartialCorrection (full = 0) or FullCorrection (full = 1) with the
+// primitive state w and the stage's dt; dx1f has nc1 entries.
+int ref_implicit_correction(const canoe_thermo_t *th, double mu_d, double cvd_R, int full,
+                            int nc3, int nc2, int nc1, int is, int ie, int js, int je, int ks,
+                            int ke, const double *dx1f, double dx2, double dx3,
+                            const double *w, double *du, double dt) {
+  try {
+    RefBlock rb(*th, mu_d, cvd_R);
+    rb.eos.reset(new EquationOfState(&rb.mb, &rb.pin));
+    rb.mb.peos = rb.eos.get();
+    rb.mb.is = is;
+    rb.mb.ie = ie;
+    rb.mb.js = js;
+    rb.mb.je = je;
+    rb.mb.ks = ks;
+    rb.mb.ke = ke;
+    rb.co.dx1f.NewAthenaArray(nc1);
+    for (int i = 0; i < nc1; ++i) rb.co.dx1f(i) = dx1f[i];
+    rb.co.dx2f.NewAthenaArray(nc2);
+    for (int j = 0; j < nc2; ++j) rb.co.dx2f(j) = dx2;
+    rb.co.dx3f.NewAthenaArray(nc3);
+    for (int k = 0; k < nc3; ++k) rb.co.dx3f(k) = dx3;
+    rb.hy.w.InitWithShallowSlice(const_cast<double *>(w), NHYDRO, nc3, nc2, nc1);
+    gi_nc1 = nc1;
+    gi_nc2 = nc2;
+    gi_nc3 = nc3;
+    ImplicitSolver solver(&rb.mb, nullptr);
+    const size_t n = (size_t)NHYDRO * nc3 * nc2 * nc1;
+    std::memcpy(g_du->data(), du, n * sizeof(double));
+    for (int k = ks; k <= ke; ++k)
+      for (int j = js; j <= je; ++j) {
+        if (full)
+          solver.FullCorrection(*g_du, rb.hy.w, dt, k, j, is, ie);
+        else
+          solver.PartialCorrection(*g_du, rb.hy.w, dt, k, j, is, ie);
+      }
+    std::memcpy(du, g_du->data(), n * sizeof(double));
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+  return 0;
+}
+
+const char *ref_last_error() { return g_err.c_str(); }
+int ref_nhydro() { return NHYDRO; }
+
+}  // extern "C"
+#endif  // REF_UNIT_IMPLICIT

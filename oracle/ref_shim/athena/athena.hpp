@@ -29,5 +29,6 @@ enum { IM1 = IVX, IM2 = IVY, IM3 = IVZ, IEN = IPR };
 constexpr Real float_min{std::numeric_limits<float>::min()};
 
 enum class TaskStatus { fail, success, next };
+enum CoordinateDirection { X1DIR = 0, X2DIR = 1, X3DIR = 2 };
 
 #include "athena_arrays.hpp"

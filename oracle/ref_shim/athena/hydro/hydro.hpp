@@ -15,6 +15,7 @@ class Hydro {
  public:
   MeshBlock *pmy_block = nullptr;
   HydroSourceTerms hsrc;
+  AthenaArray<Real> w;  // primitive state (the species correction reads it)
   void RiemannSolver(const int k, const int j, const int il, const int iu, const int ivx,
                      AthenaArray<Real> &wl, AthenaArray<Real> &wr, AthenaArray<Real> &flx,
                      const AthenaArray<Real> &dxw);

@@ -9,11 +9,21 @@
 class Coordinates;
 class EquationOfState;
 class Hydro;
+class MeshBlock;
+
+// the mesh's block lookup, reached only by neighbour exchanges a single
+// block never makes
+class Mesh {
+ public:
+  MeshBlock *FindMeshBlock(int) { return nullptr; }
+};
 
 class MeshBlock {
  public:
   class Impl;
   std::shared_ptr<Impl> pimpl;
+  Mesh *pmy_mesh = nullptr;
+  int gid = 0;
   Coordinates *pcoord = nullptr;
   EquationOfState *peos = nullptr;
   Hydro *phydro = nullptr;

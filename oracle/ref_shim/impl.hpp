@@ -7,10 +7,12 @@
 #include <snap/eos/ideal_moist.hpp>
 
 class CubedSphere;
+class ImplicitSolver;
 
 class MeshBlock::Impl {
  public:
   AthenaArray<Real> du;
   std::shared_ptr<snap::IdealMoistImpl> peos;
   std::shared_ptr<CubedSphere> pexo3;
+  std::shared_ptr<ImplicitSolver> phevi;
 };

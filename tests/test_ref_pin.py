@@ -4,12 +4,15 @@ oracle/_ref holds the reference's src/snap/riemann/lmars.cpp,
 src/snap/riemann/hllc_transform.cpp (Cartesian branch),
 src/snap/eos/ideal_moist_hydro.cpp (SoundSpeed), src/interface/eos.hpp
 (get_gamma, get_rd, get_gammad) and
-src/snap/decomposition/change_to_temperature.cpp, compiled as they lie
-against shim headers (oracle/ref_shim) for the libraries they include.  These
-tests hold the oracle's restatement to that code on seeded inputs: the
-Riemann fluxes of dry and moist face states in all three directions, the
-hydrostatic decomposition of whole C1- and C2-like blocks under every x1
-boundary pairing, and its inverse on the face states.
+src/snap/decomposition/change_to_temperature.cpp and
+src/snap/implicit/{partial,full}_correction.cpp (with forward_backward.hpp
+and flux_decomposition.hpp), compiled as they lie against shim headers
+(oracle/ref_shim) for the libraries they include.  These tests hold the
+oracle's restatement to that code on seeded inputs: the Riemann fluxes of
+dry and moist face states in all three directions, the hydrostatic
+decomposition of whole C1- and C2-like blocks under every x1 boundary
+pairing and its inverse on the face states, and the implicit vertical
+correction (3x3 and 5x5 block rows, Thomas sweep, species correction).
 
 Tolerance: both sides are compiled by the same g++ with the same
 floating-point flags (no FMA contraction) and evaluate the same formulas;
@@ -198,3 +201,50 @@ def test_pin_detects_a_planted_error():
     bad.gammad = th.gammad * (1.0 + 1e-9)
     fo = oracle.riemann(RS_HLLC, bad, ivx, wl, wr)
     assert not all(_close(fo[n], fr[n])[0] for n in range(fo.shape[0]))
+
+
+@pytest.mark.parametrize("flag", [1, 9], ids=["partial3x3", "full5x5"])
+@pytest.mark.parametrize("name,make,mu", _blocks(), ids=[b[0] for b in _blocks()])
+def test_implicit_correction_matches_reference(flag, name, make, mu):
+    """ImplicitSolver::PartialCorrection / FullCorrection (the reference's
+    Eigen code, inverses from the shim) against the oracle's block solve on
+    a perturbed state and a seeded du.  Tolerance, relative L2 per variable:
+    the two sides form the same block rows and eliminate in the same
+    (Thomas) order; they differ in how each block inverse is evaluated.  The
+    3x3 inverses are both adjugates (measured <= 5e-16: 1e-14); the 5x5 ones
+    Gauss-Jordan with partial pivoting, whose roundoff the blocks' spread of
+    scale (1/dt against c^2 rho terms) amplifies (measured <= 1e-11:
+    1e-10)."""
+    p = make()
+    p.cfg.implicit_flag = flag
+    ob = oracle.OracleBlock(p)
+    rng = np.random.Generator(np.random.PCG64(11))
+    w = ob.primitive()
+    w *= 1.0 + 1e-3 * rng.uniform(-1.0, 1.0, w.shape)
+    ob.set_primitive(w)
+    th = p.cfg.thermo
+    nv, nc3, nc2, nc1 = w.shape
+    du = np.zeros(w.shape)
+    p.interior(du)[...] = 1e-3 * rng.standard_normal(p.interior(du).shape) * \
+        np.abs(p.interior(p.u)).mean(axis=(1, 2, 3))[:, None, None, None]
+    dt = 0.3
+    got = ob.solve_implicit(du, dt)
+    is_, ie = NGHOST, NGHOST + p.cfg.nx1 - 1
+    ks, ke = (NGHOST, NGHOST + p.cfg.nx3 - 1) if p.cfg.nx3 > 1 else (0, 0)
+    js, je = (NGHOST, NGHOST + p.cfg.nx2 - 1) if p.cfg.nx2 > 1 else (0, 0)
+    x1f = np.zeros(nc1 + 1)
+    x1f[is_:ie + 2] = p.x1f
+    for g in range(1, NGHOST + 1):
+        x1f[is_ - g] = 2 * x1f[is_] - x1f[is_ + g]
+        x1f[ie + 1 + g] = 2 * x1f[ie + 1] - x1f[ie + 1 - g]
+    ref_du = ref.implicit_correction(th, mu, 1.0 / (th.gammad - 1.0), flag & 8, w, du,
+                                     np.diff(x1f), p.cfg.dx2, p.cfg.dx3, is_, ie, js, je, ks,
+                                     ke, dt)
+    a, b = p.interior(got), p.interior(ref_du)
+    tol = 1e-14 if flag == 1 else 1e-10
+    top = max(np.linalg.norm(b[n]) for n in range(nv))
+    for n in range(nv):
+        err = np.linalg.norm(a[n] - b[n]) / max(np.linalg.norm(b[n]), 1e-12 * top)
+        assert err < tol, (name, flag, n, err)
+    # and the correction did change du
+    assert np.linalg.norm(p.interior(ref_du - du)) > 1e-6 * np.linalg.norm(p.interior(du))
