@@ -436,10 +436,6 @@ def full5x5_report(args, net, steps=5, warmup=2):
     FullCorrection of most of the reference's example inputs): mixed +
     learned against plain FP64, whole steps and the x1 pencil per launch."""
     import torch
-    if world > 1:
-        run_partitioned(args, dist, rank, world)
-        return
-
     from canoe_b200 import MeshBlock
     from canoe_b200._abi import FP32_PERTURBATION, FP64, check, load
     lib = load()
