@@ -124,6 +124,22 @@ def bubble2d(nx1=150, nx2=100, x1max=1500.0, x2max=1000.0, dT=0.5, xc=500.0,
     return Problem("C1-bubble2d", cfg, x1f, u, w, dict(dt_hint=None))
 
 
+def robert2d(nx1=300, nx2=200, recon=RECON_PPM):
+    """The rising-bubble regression run of examples/2019-Li-snap/robert2d.inp:
+    300 x 200 cells on 1500 m x 1000 m, Ts = 303.15 K, bubble radius a =
+    50 m with a Gaussian skirt s = 100 m centred at (x, z) = (500, 260) m,
+    dT = 0.5 K, g = 9.8 m/s^2, p0 = 1e5 Pa, Courant number 0.9 (0.45 per
+    direction, see bubble2d), run to tlim = 1080 s with outputs every 180 s.
+    The input's fifth-order horizontal reconstruction (xorder = 5) is
+    replaced by PPM."""
+    p = bubble2d(nx1=nx1, nx2=nx2, x1max=1.5e3, x2max=1.0e3, dT=0.5, xc=500.0, zc=260.0,
+                 s=100.0, a=50.0, Ts=303.15, p0=1.0e5, grav=9.8, gamma=1.4, cfl=0.45,
+                 recon=recon)
+    p.name = "robert2d"
+    p.meta.update(tlim=1080.0, out_dt=180.0, p0=1.0e5)
+    return p
+
+
 def moist_profile(th, z, Ts=300.0, Ttop=200.0, ps=1.0e5, rh=0.8, zmoist=10.0e3,
                   nsub=16):
     """Horizontally uniform moist column at heights z (cell centres):
