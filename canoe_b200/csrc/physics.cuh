@@ -59,17 +59,18 @@ __device__ __forceinline__ R ppm_slope(R qm, R q0, R qp) {
   return copysign(lim, dwc);
 }
 
-// PPM face values of cell c from cells c-2..c+2, uniform spacing: eq. 1.6
-// face interpolation and the eq. 1.10 parabola limiter of CW84.
+// PPM interface value between cells a and b (eq. 1.6) from their values
+// and limited slopes
 template <typename R>
-__device__ __forceinline__ void ppm_cell(R qmm, R qm, R q0, R qp, R qpp, R &wL,
-                                         R &wR) {
-  R dm_m = ppm_slope(qmm, qm, q0);
-  R dm_0 = ppm_slope(qm, q0, qp);
-  R dm_p = ppm_slope(q0, qp, qpp);
+__device__ __forceinline__ R ppm_face(R qa, R qb, R dma, R dmb) {
   constexpr R sixth = R(1) / R(6);
-  wL = R(0.5) * (qm + q0) - (dm_0 - dm_m) * sixth;
-  wR = R(0.5) * (q0 + qp) - (dm_p - dm_0) * sixth;
+  return R(0.5) * (qa + qb) - (dmb - dma) * sixth;
+}
+
+// the eq. 1.10 parabola limiter of CW84 on cell value q0 and its
+// interface values wL, wR
+template <typename R>
+__device__ __forceinline__ void ppm_limit(R q0, R &wL, R &wR) {
   if ((wR - q0) * (q0 - wL) <= R(0)) {
     wL = q0;
     wR = q0;
@@ -81,6 +82,19 @@ __device__ __forceinline__ void ppm_cell(R qmm, R qm, R q0, R qp, R qpp, R &wL,
     else if (-d * d > d * m6)
       wR = R(3) * q0 - R(2) * wL;
   }
+}
+
+// PPM face values of cell c from cells c-2..c+2, uniform spacing: eq. 1.6
+// face interpolation and the eq. 1.10 parabola limiter of CW84.
+template <typename R>
+__device__ __forceinline__ void ppm_cell(R qmm, R qm, R q0, R qp, R qpp, R &wL,
+                                         R &wR) {
+  R dm_m = ppm_slope(qmm, qm, q0);
+  R dm_0 = ppm_slope(qm, q0, qp);
+  R dm_p = ppm_slope(q0, qp, qpp);
+  wL = ppm_face(qm, q0, dm_m, dm_0);
+  wR = ppm_face(q0, qp, dm_0, dm_p);
+  ppm_limit(q0, wL, wR);
 }
 
 // PLM with the van Leer (1979) harmonic-mean limiter, uniform spacing.
