@@ -491,6 +491,73 @@ __global__ void k_shell_edges(const double *__restrict__ w, const EdgeRow *__res
 
 constexpr int TI = 32, TD = 8;
 
+// the x2 (DIR 1) / x3 (DIR 2) flux at the face of table index kj from its
+// left / right states (overwritten): PrimToLocal2/3, HLLC, FluxToGlobal2/3
+// and the covariant projection
+template <int DIR, typename R>
+__device__ __forceinline__ void shell_face_flux(const Geom &g, const canoe_thermo_t &th,
+                                                R *wl, R *wr, double pref, int64_t kj,
+                                                int64_t nkj, double *fx) {
+  constexpr bool PERT = sizeof(R) == 4;
+  R fr[kNV];
+  if (DIR == 1) {
+    // PrimToLocal2 with Face2Metric: T22 = 1/sqrt(gi22), T32 = g23/sqrt(g33)
+    const double ct = g.shell[kTabCosF2 * nkj + kj], st = g.shell[kTabSinF2 * nkj + kj];
+    const double gi22 = 1.0 / (st * st);
+    const double T22 = 1.0 / sqrt(gi22), T32 = ct / sqrt(1.0), T33 = sqrt(1.0);
+    auto loc = [&](R *x) {
+      const R u2 = x[2], u3 = x[3];
+      x[2] = R(T22) * u2;
+      x[3] = R(T32) * u2 + R(T33) * u3;
+    };
+    loc(wl);
+    loc(wr);
+    if constexpr (PERT)
+      hllc_pert<R, 0, 1>(th, wl, wr, R(pref), fr);
+    else
+      hllc<R, 0, 1>(th, wl, wr, fr);
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) fx[n] = fr[n];
+    if (PERT) fx[2] += pref;
+    const double F22 = sqrt(gi22), F32 = -sqrt(gi22) * ct / 1.0, F33 = 1.0 / sqrt(1.0);
+    const double txy = fx[2], txz = fx[3];
+    fx[2] = F22 * txy;
+    fx[3] = F32 * txy + F33 * txz;
+    const double cth = g.shell[kTabCth2 * nkj + kj];
+    const double ty_ = fx[2], tz_ = fx[3];
+    fx[2] = ty_ + tz_ * cth;
+    fx[3] = tz_ + ty_ * cth;
+  } else {
+    // PrimToLocal3 with Face3Metric: T22 = sqrt(g22), T23 = g23/sqrt(g22),
+    // T33 = 1/sqrt(gi33)
+    const double ct = g.shell[kTabCosF3 * nkj + kj], st = g.shell[kTabSinF3 * nkj + kj];
+    const double gi33 = 1.0 / (st * st);
+    const double T22 = sqrt(1.0), T23 = ct / sqrt(1.0), T33 = 1.0 / sqrt(gi33);
+    auto loc = [&](R *x) {
+      const R u2 = x[2], u3 = x[3];
+      x[2] = R(T22) * u2 + R(T23) * u3;
+      x[3] = R(T33) * u3;
+    };
+    loc(wl);
+    loc(wr);
+    if constexpr (PERT)
+      hllc_pert<R, 0, 2>(th, wl, wr, R(pref), fr);
+    else
+      hllc<R, 0, 2>(th, wl, wr, fr);
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) fx[n] = fr[n];
+    if (PERT) fx[3] += pref;
+    const double F22 = 1.0 / sqrt(1.0), F23 = -ct / 1.0 * sqrt(gi33), F33 = sqrt(gi33);
+    const double txy = fx[2], txz = fx[3];
+    fx[2] = F22 * txy + F23 * txz;
+    fx[3] = F33 * txz;
+    const double cth = g.shell[kTabCth3 * nkj + kj];
+    const double ty_ = fx[2], tz_ = fx[3];
+    fx[2] = ty_ + tz_ * cth;
+    fx[3] = tz_ + ty_ * cth;
+  }
+}
+
 // x2 (DIR 1) / x3 (DIR 2) fluxes and their divergence on (32 i) x (8 cells)
 // tiles; blockIdx.z runs over panel x rows.  R = float: reconstruction and
 // the Riemann solver in FP32 on p' = p - pref(i); the metric transforms, the
@@ -562,7 +629,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
   __syncthreads();
   for (int f = ty; f <= nd; f += blockDim.y) {
     const int fd = d0 + f;
-    R wl[kNV], wr[kNV], fr[kNV];
+    R wl[kNV], wr[kNV];
     double fx[kNV];
 #pragma unroll
     for (int n = 0; n < kNV; ++n) {
@@ -585,62 +652,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
     }
     const int kf = DIR == 1 ? o : fd, jf = DIR == 1 ? fd : o;
     const int64_t kj = (int64_t)kf * g.nc2 + jf;
-    if (DIR == 1) {
-      // PrimToLocal2 with Face2Metric: T22 = 1/sqrt(gi22), T32 = g23/sqrt(g33)
-      const double ct = g.shell[kTabCosF2 * nkj + kj], st = g.shell[kTabSinF2 * nkj + kj];
-      const double gi22 = 1.0 / (st * st);
-      const double T22 = 1.0 / sqrt(gi22), T32 = ct / sqrt(1.0), T33 = sqrt(1.0);
-      auto loc = [&](R *x) {
-        const R u2 = x[2], u3 = x[3];
-        x[2] = R(T22) * u2;
-        x[3] = R(T32) * u2 + R(T33) * u3;
-      };
-      loc(wl);
-      loc(wr);
-      if constexpr (PERT)
-        hllc_pert<R, 0, 1>(th, wl, wr, R(pref), fr);
-      else
-        hllc<R, 0, 1>(th, wl, wr, fr);
-#pragma unroll
-      for (int n = 0; n < kNV; ++n) fx[n] = fr[n];
-      if (PERT) fx[2] += pref;
-      const double F22 = sqrt(gi22), F32 = -sqrt(gi22) * ct / 1.0, F33 = 1.0 / sqrt(1.0);
-      const double txy = fx[2], txz = fx[3];
-      fx[2] = F22 * txy;
-      fx[3] = F32 * txy + F33 * txz;
-      const double cth = g.shell[kTabCth2 * nkj + kj];
-      const double ty_ = fx[2], tz_ = fx[3];
-      fx[2] = ty_ + tz_ * cth;
-      fx[3] = tz_ + ty_ * cth;
-    } else {
-      // PrimToLocal3 with Face3Metric: T22 = sqrt(g22), T23 = g23/sqrt(g22),
-      // T33 = 1/sqrt(gi33)
-      const double ct = g.shell[kTabCosF3 * nkj + kj], st = g.shell[kTabSinF3 * nkj + kj];
-      const double gi33 = 1.0 / (st * st);
-      const double T22 = sqrt(1.0), T23 = ct / sqrt(1.0), T33 = 1.0 / sqrt(gi33);
-      auto loc = [&](R *x) {
-        const R u2 = x[2], u3 = x[3];
-        x[2] = R(T22) * u2 + R(T23) * u3;
-        x[3] = R(T33) * u3;
-      };
-      loc(wl);
-      loc(wr);
-      if constexpr (PERT)
-        hllc_pert<R, 0, 2>(th, wl, wr, R(pref), fr);
-      else
-        hllc<R, 0, 2>(th, wl, wr, fr);
-#pragma unroll
-      for (int n = 0; n < kNV; ++n) fx[n] = fr[n];
-      if (PERT) fx[3] += pref;
-      const double F22 = 1.0 / sqrt(1.0), F23 = -ct / 1.0 * sqrt(gi33), F33 = sqrt(gi33);
-      const double txy = fx[2], txz = fx[3];
-      fx[2] = F22 * txy + F23 * txz;
-      fx[3] = F33 * txz;
-      const double cth = g.shell[kTabCth3 * nkj + kj];
-      const double ty_ = fx[2], tz_ = fx[3];
-      fx[2] = ty_ + tz_ * cth;
-      fx[3] = tz_ + ty_ * cth;
-    }
+    shell_face_flux<DIR, R>(g, th, wl, wr, pref, kj, nkj, fx);
 #pragma unroll
     for (int n = 0; n < kNV; ++n) F[n][f][tx] = fx[n];
     if constexpr (WF) {
@@ -686,6 +698,175 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
     }
   }
 }
+
+// The same fluxes with one thread per (i, o, run of SRL cells) marching
+// along the flux direction with its stencil in registers, as
+// k_flux_x23_run in flux.cu: each step reconstructs one cell (PPM slopes
+// and interface values streamed once per cell), takes the swapped state at
+// a panel edge, computes the flux at the cell's lower face and finishes the
+// divergence of the cell below.  blockIdx.z runs over panel x runs.  Same
+// expressions on the same operands as the tile kernel: the same bits.
+constexpr int SRL = 16;  // cells per run
+constexpr int SBY = 4;   // orthogonal lines per CTA
+
+template <int RECON, int DIR, bool WF, typename R>
+__global__ void __launch_bounds__(32 * SBY)
+    k_shell_flux_x23_run(Geom g, canoe_thermo_t th, const double *__restrict__ w,
+                         double *__restrict__ du, const double *__restrict__ dtp, double beta,
+                         int64_t pvals, const double *__restrict__ lr,
+                         double *__restrict__ fout) {
+  constexpr bool PERT = sizeof(R) == 4;
+  const int N = g.nx2;
+  const int nrun = (N + SRL - 1) / SRL;
+  const int p = blockIdx.z / nrun;
+  const int i = g.is + blockIdx.x * 32 + threadIdx.x;
+  const int o = (DIR == 1 ? g.ks : g.js) + blockIdx.y * SBY + threadIdx.y;
+  if (i > g.ie || o > (DIR == 1 ? g.ke : g.je)) return;
+  const int dlo = DIR == 1 ? g.js : g.ks, dhi = DIR == 1 ? g.je : g.ke;
+  const int s0 = dlo + (int)(blockIdx.z % nrun) * SRL;
+  const int s1 = min(s0 + SRL, dhi + 1);  // one past the run's last cell
+  const int64_t sd = DIR == 1 ? g.nc1 : g.sk;
+  const int64_t pb = p * pvals;
+  const int64_t base = pb + (DIR == 1 ? (int64_t)o * g.sk : (int64_t)o * g.nc1) + i;
+  const int64_t nkj = (int64_t)g.nc3 * g.nc2;
+  const double pref = PERT ? g.pref[i] : 0.;
+  const double wght = beta * dtp[0];
+  const double xv = g.x1v[i], df = g.dx1f[i];
+  const int pos = o - (DIR == 1 ? g.ks : g.js);
+  constexpr int H = RECON == CANOE_RECON_PPM ? 2 : 1;
+
+  R q[3][kNV];  // PLM: cells c-1, c, c+1; PPM: c, c+1, c+2
+  R sl[kNV], fl[kNV];
+  double nx[kNV];
+  auto fetch = [&](int c) {
+    const int64_t off = base + (int64_t)c * sd;
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) nx[n] = w[n * g.sv + off];
+  };
+  auto put = [&](R *qm) {
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) {
+      double v = nx[n];
+      if (PERT && n == 4) v -= pref;
+      qm[n] = R(v);
+    }
+  };
+  if constexpr (RECON == CANOE_RECON_PPM) {
+    R qa[kNV], qb[kNV];
+    fetch(s0 - 3);
+    put(qa);
+    fetch(s0 - 2);
+    put(qb);
+    fetch(s0 - 1);
+    put(q[0]);
+    fetch(s0);
+    put(q[1]);
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) {
+      const R sb = ppm_slope(qa[n], qb[n], q[0][n]);
+      sl[n] = ppm_slope(qb[n], q[0][n], q[1][n]);
+      fl[n] = ppm_face(qb[n], q[0][n], sb, sl[n]);
+    }
+  } else {
+    fetch(s0 - 2);
+    put(q[0]);
+    fetch(s0 - 1);
+    put(q[1]);
+  }
+  fetch(s0 - 1 + H);
+  R wrp[kNV];
+  double fp[kNV], dpre[kNV];
+  double amp = 0.;  // lower-face area of the cell below the current face
+  for (int c = s0 - 1; c <= s1; ++c) {
+    put(q[2]);
+    if (c < s1) fetch(c + H + 1);  // one step ahead
+    if (DIR == 2 && c > s0) {
+      const int64_t off = base + (int64_t)(c - 1) * sd;
+#pragma unroll
+      for (int n = 0; n < kNV; ++n) dpre[n] = du[n * g.sv + off];
+    }
+    R wlc[kNV], wrc[kNV];
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) {
+      if constexpr (RECON == CANOE_RECON_PPM) {
+        const R sr = ppm_slope(q[0][n], q[1][n], q[2][n]);
+        const R fr = ppm_face(q[0][n], q[1][n], sl[n], sr);
+        wlc[n] = fl[n];
+        wrc[n] = fr;
+        ppm_limit(q[0][n], wlc[n], wrc[n]);
+        sl[n] = sr;
+        fl[n] = fr;
+      } else {
+        plm_cell(q[0][n], q[1][n], q[2][n], wlc[n], wrc[n]);
+      }
+    }
+    if (c >= s0) {
+      // face c: left = wR of cell c-1, right = wL of cell c; at a panel edge
+      // the ghost side is the neighbour's swapped state
+      R wl[kNV], wr[kNV];
+#pragma unroll
+      for (int n = 0; n < kNV; ++n) {
+        wl[n] = wrp[n];
+        wr[n] = wlc[n];
+      }
+      if (c == dlo) {
+        const double *s = lr + ((((int64_t)p * 4 + (DIR == 1 ? 0 : 2)) * N + pos) * kNV) * g.nx1 +
+                          (i - g.is);
+#pragma unroll
+        for (int n = 0; n < kNV; ++n) wl[n] = R(s[(int64_t)n * g.nx1]);
+      }
+      if (c == dhi + 1) {
+        const double *s = lr + ((((int64_t)p * 4 + (DIR == 1 ? 1 : 3)) * N + pos) * kNV) * g.nx1 +
+                          (i - g.is);
+#pragma unroll
+        for (int n = 0; n < kNV; ++n) wr[n] = R(s[(int64_t)n * g.nx1]);
+      }
+      const int kf = DIR == 1 ? o : c, jf = DIR == 1 ? c : o;
+      const int64_t kj = (int64_t)kf * g.nc2 + jf;
+      double fx[kNV];
+      shell_face_flux<DIR, R>(g, th, wl, wr, pref, kj, nkj, fx);
+      if constexpr (WF) {
+#pragma unroll
+        for (int n = 0; n < kNV; ++n) {
+          const int64_t idx =
+              DIR == 1 ? (((int64_t)(p * kNV + n) * g.nc3 + o) * (g.nc2 + 1) + c) * g.nc1 + i
+                       : (((int64_t)(p * kNV + n) * (g.nc3 + 1) + c) * g.nc2 + o) * g.nc1 + i;
+          fout[idx] = fx[n];
+        }
+      }
+      // this face's area: the upper face of cell c-1, the lower one of c
+      const double ac = DIR == 1 ? xv * g.shell[kTabDx3AF2 * nkj + kj] * df
+                                 : xv * g.shell[kTabDx2AF3 * nkj + kj] * df;
+      if (c > s0) {
+        const int kc = DIR == 1 ? o : c - 1, jc = DIR == 1 ? c - 1 : o;
+        const int64_t kjc = (int64_t)kc * g.nc2 + jc;
+        const double d2 = g.shell[kTabDx2A * nkj + kjc], d3 = g.shell[kTabDx3A * nkj + kjc];
+        const double vol = df * d2 * d3 * xv * xv * g.shell[kTabSinC * nkj + kjc];
+        const int64_t off = base + (int64_t)(c - 1) * sd;
+#pragma unroll
+        for (int n = 0; n < kNV; ++n) {
+          const double dfl = ac * fx[n] - amp * fp[n];
+          if (DIR == 1)
+            du[n * g.sv + off] = -(wght * dfl / vol);
+          else
+            du[n * g.sv + off] = dpre[n] - wght * dfl / vol;
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < kNV; ++n) fp[n] = fx[n];
+      amp = ac;
+    }
+#pragma unroll
+    for (int n = 0; n < kNV; ++n) {
+      wrp[n] = wrc[n];
+      q[0][n] = q[1][n];
+      q[1][n] = q[2][n];
+    }
+  }
+}
+
+// 1: the panel x2 / x3 fluxes run as k_shell_flux_x23_run, 0: as tiles
+constexpr int kShellFluxRun = 1;
 
 }  // namespace
 }  // namespace cb
@@ -761,6 +942,24 @@ static int shell_edges(canoe_shell *s) {
 template <typename R>
 static int shell_x23_t(canoe_shell *s, int dir, double beta, double *fout) {
   const Geom &g = s->g;
+  const bool ppm = s->cfg.recon == CANOE_RECON_PPM;
+  if constexpr (kShellFluxRun != 0) {
+    dim3 rgrid((g.nx1 + 31) / 32, (g.nx2 + SBY - 1) / SBY, 6 * ((g.nx2 + SRL - 1) / SRL));
+    dim3 rblk(32, SBY);
+#define CB_SR(RC, D, W)                                                              \
+  k_shell_flux_x23_run<RC, D, W, R><<<rgrid, rblk, 0, s->st>>>(                      \
+      g, s->th, s->d_w, s->d_du, s->d_dt, beta, s->pvals, s->d_lr, fout)
+    if (dir == 1) {
+      if (ppm) { if (fout) CB_SR(3, 1, true); else CB_SR(3, 1, false); }
+      else { if (fout) CB_SR(2, 1, true); else CB_SR(2, 1, false); }
+    } else {
+      if (ppm) { if (fout) CB_SR(3, 2, true); else CB_SR(3, 2, false); }
+      else { if (fout) CB_SR(2, 2, true); else CB_SR(2, 2, false); }
+    }
+#undef CB_SR
+    CB_CUDA(cudaGetLastError());
+    return 0;
+  }
   dim3 grid((g.nx1 + TI - 1) / TI, (g.nx2 + TD - 1) / TD, 6 * g.nx2);
   dim3 blk(TI, 8);
   const size_t tiles = sizeof(R) * kNV * TI * ((TD + 2 * NG) + 2 * (TD + 2));
@@ -768,7 +967,6 @@ static int shell_x23_t(canoe_shell *s, int dir, double beta, double *fout) {
 #define CB_SX(RC, D, W)                                                                   \
   k_shell_flux_x23<RC, D, W, R><<<grid, blk, smem, s->st>>>(g, s->th, s->d_w, s->d_du,    \
                                                             s->d_dt, beta, s->pvals, s->d_lr, fout)
-  const bool ppm = s->cfg.recon == CANOE_RECON_PPM;
   if (dir == 1) {
     if (ppm) { if (fout) CB_SX(3, 1, true); else CB_SX(3, 1, false); }
     else { if (fout) CB_SX(2, 1, true); else CB_SX(2, 1, false); }
