@@ -213,13 +213,28 @@ __device__ __forceinline__ void sat_eval(const canoe_thermo_t &th, const SatCell
   fp = c.rho * (cvd * cvs + dlat);
 }
 
+// true when no liquid or ice slot of the cell holds water
+template <int NY>
+__device__ __forceinline__ bool all_vapour(const canoe_thermo_t &th, const double *q) {
+  bool dry = true;
+#pragma unroll
+  for (int v = 0; v < (NY > 0 ? NY : 1); ++v) {
+    if (v >= th.nvapor) break;
+#pragma unroll
+    for (int n = 1; n <= NY; ++n)
+      if ((n == th.liq_slot[v] || n == th.ice_slot[v]) && q[n] != 0.) dry = false;
+  }
+  return dry;
+}
+
 // a guess below this much latent heating [K] keeps the cold start, which is
 // exact in one step for cells that stay unsaturated
 constexpr double kSatGate = 0.05;
 
 // returns the number of f evaluations; flags bit0 fallback, bit1 not
-// converged.  Start (o.warm): 0 the unadjusted temperature (cold); 1 the
-// guess; 2 gated: the guess if it exceeds the cold start by kSatGate.
+// converged, bit2 the cell is returned unchanged (no write needed).  Start
+// (o.warm): 0 the unadjusted temperature (cold); 1 the guess; 2 gated: the
+// guess if it exceeds the cold start by kSatGate.
 template <int NY>
 __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                         double *uc, double t_guess, double &t_out, int &flags) {
@@ -293,9 +308,21 @@ __device__ int sat_cell(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
   double qn[NY + 1];
   // gated start: the guess when it predicts latent heating, else cold
   if (o.warm == 2 && guess_ok && t_guess - t_cold > kSatGate) T = t_guess;
+  // a cell whose water is all vapour and that stays below saturation at
+  // the cold start is already the equilibrium: Newton would end where it
+  // starts (to about 1e-13 K) and write the vapour back through a density
+  // round trip, so the first evaluation returns it unchanged (flags bit 2)
+  const bool dry_in = all_vapour<NY>(th, q);
   const int it0 = 0;
   for (int it = it0; it < o.max_iter && !converged; ++it) {
     sat_eval<NY>(th, c, T, -1, 0, f, fp, qn);
+    if (it == 0 && dry_in && T == t_cold) {
+      if (all_vapour<NY>(th, qn)) {
+        t_out = t_cold;
+        flags = 4;
+        return 1;
+      }
+    }
     if (!(fabs(f) < fprev) && it > 0) {
       fallback = true;
       break;
@@ -476,12 +503,12 @@ __global__ void __launch_bounds__(256, 3)
     for (int n = 0; n < S::NV; ++n) uc[n] = u[n * stride + off];
   }
   double tg = t_guess && active ? t_guess[t] : 0.;
+  double tdry = 0.;
+  bool need = false;
   if constexpr (LEARNED) {
     // every lane of the warp takes part in the tensor-core inference
     // (a warp whose cells all stay unsaturated skips the inference)
     float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f};
-    double tdry = 0.;
-    bool need = false;
     if (active) {
       tdry = mlp_features<NY>(th, uc, x);
       need = may_condense<NY>(th, uc, tdry);
@@ -509,11 +536,22 @@ __global__ void __launch_bounds__(256, 3)
     }
     if (guess_out && active) guess_out[t] = tg;
   }
-  if (active) {
+  // the learned start's screen (may_condense, with its 1e-3 margin) also
+  // decides the cells that stay all vapour: a warp whose cells are all such
+  // ends here, as sat_cell's first evaluation would end them
+  bool skip = false;
+  if constexpr (LEARNED)
+    skip = __all_sync(0xffffffffu, !active || (!need && all_vapour<NY>(th, uc)));
+  if (skip) {
+    if (active && t_out) t_out[t] = tdry;
+    if (active && iters) iters[t] = 0;
+  } else if (active) {
     double T;
     it = sat_cell<NY>(th, o, uc, tg, T, fl);
+    if (!(fl & 4)) {
 #pragma unroll
-    for (int n = 1; n <= NY; ++n) u[n * stride + off] = uc[n];
+      for (int n = 1; n <= NY; ++n) u[n * stride + off] = uc[n];
+    }
     if (t_out) t_out[t] = T;
     if (iters) iters[t] = it;
   }
