@@ -307,8 +307,12 @@ int run_x23(const Geom &g, const canoe_thermo_t &th, const double *w, double *du
             const double *dtp, double beta, double *fo, cudaStream_t st) {
   const int nd = DIR == 1 ? g.nx2 : g.nx3;
   const int no = DIR == 1 ? g.nx3 : g.nx2;
-  if constexpr (kFluxRun != 0) {
-    constexpr int RL = run_len<R>();
+  constexpr int RL = run_len<R>();
+  // a 2-D block (one line across the flux direction) keeps the tile kernel:
+  // its runs would fill one warp in four of each CTA, and the 150 x 100
+  // bubble would march 20 warps in all (x2 pass 4 x slower than the tiles);
+  // thin 3-D blocks keep the runs, whose launches overlap in a batch
+  if (kFluxRun != 0 && no >= RBY) {
     dim3 grid((g.nx1 + 31) / 32, (no + RBY - 1) / RBY, (nd + RL - 1) / RL);
     k_flux_x23_run<NY, RECON, RS, DIR, WF, R><<<grid, dim3(32, RBY), 0, st>>>(g, th, w, du, dtp,
                                                                               beta, fo);

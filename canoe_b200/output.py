@@ -213,9 +213,11 @@ class NetcdfOutput:
     (netcdf.cpp:472-476)."""
 
     def __init__(self, basename, dt, file_id="out2", variables=("prim", "uov"), p0=1.0e5,
-                 species=None, combine=True, keep_blocks=False):
+                 species=None, combine=True, keep_blocks=False, only=None):
+        """only: names of the cell variables to keep (None: all of them)."""
         self.basename, self.dt, self.file_id = basename, float(dt), file_id
         self.variables, self.p0, self.species = variables, p0, species
+        self.only = only
         self.combine, self.keep_blocks = combine, keep_blocks
         self.next_time = 0.0
         self.file_number = 0
@@ -233,9 +235,10 @@ class NetcdfOutput:
         for gid, (cfg, x1f, w, off) in enumerate(blocks):
             dec = {d: (mesh_n[d], off[d - 1]) for d in (1, 2, 3)}
             path = block_filename(self.basename, gid, self.file_id, self.file_number)
-            write_file(path, coordinates(cfg, x1f),
-                       cell_fields(cfg, w, self.variables, self.p0, self.species), time, dec,
-                       len(blocks))
+            fields = cell_fields(cfg, w, self.variables, self.p0, self.species)
+            if self.only is not None:
+                fields = {k: v for k, v in fields.items() if k in self.only}
+            write_file(path, coordinates(cfg, x1f), fields, time, dec, len(blocks))
             paths.append(path)
         out = paths
         if self.combine:

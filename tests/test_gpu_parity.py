@@ -151,6 +151,38 @@ def test_calculate_fluxes(oracle_mod, case):
         assert err < tol, f"x{d + 1} flux rel L2 {err}"
 
 
+@pytest.mark.parametrize("fp32", [False, True], ids=["fp64", "fp32"])
+def test_flux_runs_at_run_size(oracle_mod, fp32):
+    """The x2 / x3 register-window runs on a block of many runs per line
+    (the 2-D cases above take the shared-memory tiles, the 3-D ones one or
+    two runs per line): C2 physics at 128 x 112 x 112, fluxes against the
+    oracle (FP64 to the operator bar, FP32 on the perturbation to its 1e-5
+    per-variable bar) and one FP64 step."""
+    from canoe_b200._abi import FP32_PERTURBATION
+    p = perturb(problems.moist3d(nx1=128, nx2=112, nx3=112, x1max=16.0e3, x2max=28.0e3,
+                                 x3max=28.0e3, noise=0.5))
+    ora = oracle_mod.OracleBlock(p)
+    o = ora.calculate_fluxes()
+    if fp32:
+        p.cfg.precision = FP32_PERTURBATION
+    gpu = MeshBlock(p)
+    g = gpu.calculate_fluxes()
+    for d in (1, 2):
+        a, b = g[d], o[d]
+        if fp32:
+            top = max(np.linalg.norm(b[n]) for n in range(b.shape[0]))
+            err = max(rel_l2(a[n], b[n], floor=1e-6 * top) for n in range(b.shape[0]))
+            assert err < 1e-5, f"x{d + 1} flux rel L2 {err}"
+        else:
+            assert max_var_rel_l2(a, b) < OP_TOL
+    if not fp32:
+        dt = ora.new_dt()
+        ora.step(dt)
+        gpu.step(dt)
+        assert rel_l2(p.interior(gpu.conserved()), p.interior(ora.conserved())) < 1e-11
+    gpu.close()
+
+
 @pytest.mark.parametrize("case", ["c2_ppm_hllc", "c2_full5x5"])
 def test_solve_implicit(oracle_mod, case):
     p = perturb(CASES[case]())
