@@ -58,9 +58,19 @@ __global__ void __launch_bounds__(256)
   double dtc = __longlong_as_double(0x7ff0000000000000LL);
   uint32_t bits = 0;
   if (t < total) {
-    const int i = (int)(t % g.nc1);
-    const int j = (int)((t / g.nc1) % g.nc2);
-    const int k = (int)(t / g.sk);
+    // 32-bit index arithmetic where the block allows (64-bit division is
+    // several times the instructions)
+    int i, j, k;
+    if (total <= 0x7fffffff) {
+      const unsigned tt = (unsigned)t, r = tt / (unsigned)g.nc1;
+      i = (int)(tt - r * (unsigned)g.nc1);
+      j = (int)(r % (unsigned)g.nc2);
+      k = (int)(r / (unsigned)g.nc2);
+    } else {
+      i = (int)(t % g.nc1);
+      j = (int)((t / g.nc1) % g.nc2);
+      k = (int)(t / g.sk);
+    }
     bool f1 = false, f2 = false, f3 = false;
     const int si = map_ghost(i, g.is, g.ie, g.nx1, g.bc[0], g.bc[1], f1);
     const int sj = g.f2 ? map_ghost(j, g.js, g.je, g.nx2, g.bc[2], g.bc[3], f2) : j;
