@@ -61,6 +61,7 @@ META = {
     "vel3": ("horizontal velocity", "m/s"),
     "temp": ("temperature", "K"),
     "theta": ("potential temperature", "K"),
+    "theta_e": ("equivalent potential temperature", "K"),
 }
 
 # (axis letter, long name of the centres, long name of the faces) of the
@@ -131,14 +132,19 @@ def cell_fields(cfg, w, variables=("prim", "uov"), p0=1.0e5, species=None):
             out[f"vel{d + 1}"] = wi[1 + ny + d]
         for name, qn in zip(species or species_names(th), q):
             out[name] = qn
-    if "uov" in variables:
+    if "uov" in variables or "theta_e" in variables:
         feps = np.ones_like(rho)
         for n in range(ny):
             feps = feps + (q[n] * th.inv_mu_ratio_m1[n] if n < th.nvapor else -q[n])
         temp = pres / (rho * th.rd * feps)
-        chi = (th.gammad - 1.0) / th.gammad
-        out["temp"] = temp
-        out["theta"] = temp * (p0 / pres) ** chi
+        if "uov" in variables:
+            chi = (th.gammad - 1.0) / th.gammad
+            out["temp"] = temp
+            out["theta"] = temp * (p0 / pres) ** chi
+        if "theta_e" in variables:
+            # the moist bubble's output (bryan.cpp:62-90)
+            from . import thermo
+            out["theta_e"] = thermo.theta_e(th, q, temp, pres, p0)
     return out
 
 
@@ -301,6 +307,34 @@ def combine_blocks(basename, file_id, number, remove=False):
     if remove:
         for p in paths:
             os.remove(p)
+    return out
+
+
+def join_records(paths, out):
+    """One file holding the single time records of `paths` in order (the
+    reference's outputs of one run joined along time, as ncrcat does), so a
+    check can index the record of an output number."""
+    with netcdf_file(paths[0], "r", mmap=False) as f0:
+        dims = {k: v for k, v in f0.dimensions.items()}
+        meta = {k: (f0.variables[k].dimensions, f0.variables[k].typecode(),
+                    {a: getattr(f0.variables[k], a) for a in f0.variables[k]._attributes})
+                for k in f0.variables}
+        static = {k: f0.variables[k][:].copy() for k in f0.variables
+                  if "time" not in f0.variables[k].dimensions}
+    with netcdf_file(out, "w", version=1) as g:
+        for k, n in dims.items():
+            g.createDimension(k, n)
+        for k, (d, tc, attrs) in meta.items():
+            v = g.createVariable(k, tc, d)
+            for a, val in attrs.items():
+                setattr(v, a, val)
+            if k in static:
+                v[:] = static[k]
+        for r, p in enumerate(paths):
+            with netcdf_file(p, "r", mmap=False) as f:
+                for k, (d, _, _) in meta.items():
+                    if "time" in d:
+                        g.variables[k][r] = f.variables[k][0]
     return out
 
 

@@ -140,6 +140,88 @@ def robert2d(nx1=300, nx2=200, recon=RECON_PPM):
     return p
 
 
+def _solve_T(f, lo, hi, it=60):
+    """Bisection of the increasing function f on [lo, hi] (arrays)."""
+    lo, hi = np.array(lo, dtype=np.float64), np.array(hi, dtype=np.float64)
+    for _ in range(it):
+        mid = 0.5 * (lo + hi)
+        up = f(mid) > 0.0
+        hi = np.where(up, mid, hi)
+        lo = np.where(up, lo, mid)
+    return 0.5 * (lo + hi)
+
+
+def bryan2d(nx1=200, nx2=400, x1max=10.0e3, x2max=20.0e3, Ts=289.85, p0=1.0e5, qt=0.0196,
+            dT=2.0, xc=10.0e3, zc=2.0e3, xr=2.0e3, zr=2.0e3, grav=9.81, cfl=0.45,
+            recon=RECON_PPM, rsolver=RS_LMARS, nsub=16):
+    """The moist rising bubble of examples/2019-Li-snap/bryan.inp / bryan.cpp
+    (Bryan and Fritsch 2002) on the earth-moist.yaml thermo (dry air, H2O
+    vapour and liquid): a saturated reversible moist adiabat of total water
+    qt from (Ts, p0) at the ground, and a virtual-temperature bubble of dT
+    (cos^2 in the normalised distance L < 1) re-equilibrated at constant
+    pressure and total water (bryan.cpp:103-155).  The adiabat keeps the
+    moist static energy h + g z of the saturated parcel constant with
+    hydrostatic pressure, integrated with nsub midpoint steps per cell from
+    the ground to the first cell centre and on from centre to centre.
+    Courant number 0.9 split over the two directions as in bubble2d;
+    fifth-order horizontal reconstruction replaced by PPM."""
+    th = T.moist(("H2O",), ice=False, grav=-grav)
+    x1f = np.linspace(0.0, x1max, nx1 + 1)
+    z = 0.5 * (x1f[1:] + x1f[:-1])
+    dx2 = x2max / nx2
+    x2v = (np.arange(nx2) + 0.5) * dx2
+
+    def state(Tk, pk):
+        qv, ql = T.sat_split(th, Tk, pk, qt)
+        return np.array([qv, ql])
+
+    def rho_of(Tk, pk):
+        return pk / (th.rd * T.feps_of(th, state(Tk, pk)) * Tk)
+
+    H0 = T.enthalpy(th, state(Ts, p0), Ts)
+
+    def T_at(pk, zk, Tg):
+        return _solve_T(lambda t: T.enthalpy(th, state(t, pk), t) - (H0 - grav * zk),
+                        Tg - 30.0, Tg + 5.0)
+
+    Tcol, pcol = np.empty(nx1), np.empty(nx1)
+    Tk, pk, zk = Ts, p0, 0.0
+    for i in range(nx1):
+        h = (z[i] - zk) / nsub
+        for _ in range(nsub):
+            pm = pk - 0.5 * h * grav * rho_of(Tk, pk)
+            Tm = T_at(pm, zk + 0.5 * h, Tk)
+            pk = pk - h * grav * rho_of(Tm, pm)
+            zk = zk + h
+            Tk = T_at(pk, zk, Tk)
+        Tcol[i], pcol[i] = Tk, pk
+    Tt = np.broadcast_to(Tcol[None, :], (nx2, nx1)).copy()  # (j, i)
+    pp = np.broadcast_to(pcol[None, :], (nx2, nx1)).copy()
+    # virtual-temperature bubble at constant pressure and total water
+    zz, xx = np.meshgrid(z, x2v)
+    L = np.sqrt(((xx - xc) / xr) ** 2 + ((zz - zc) / zr) ** 2)
+    inb = L < 1.0
+    if inb.any():
+        t0, p_ = Tt[inb], pp[inb]
+        tv = t0 * T.feps_of(th, state(t0, p_)) * (1.0 + dT * np.cos(np.pi * L[inb] / 2.0) ** 2 / 300.0)
+        Tt[inb] = _solve_T(lambda t: t * T.feps_of(th, state(t, p_)) - tv, t0, t0 + dT * Ts / 300.0)
+    q = state(Tt, pp)
+    rho = pp / (th.rd * T.feps_of(th, q) * Tt)
+    nv = 5 + th.ny
+    w_int = np.zeros((nv, 1, nx2, nx1))
+    w_int[0, 0] = rho
+    w_int[1, 0], w_int[2, 0] = q[0], q[1]
+    w_int[4 + th.ny, 0] = pp
+    shape = _shape(nx1, nx2, 1, nv)
+    w = _embed(shape, w_int, nx1, nx2, 1)
+    u = _embed(shape, T.prim_to_cons(th, w_int), nx1, nx2, 1)
+    bc = [BC_REFLECT] * 4 + [BC_PERIODIC] * 2
+    cfg, x1f = make_config(nx1, nx2, 1, x1f, dx2, 1.0, th, bc, recon, rsolver,
+                           implicit_flag=0, satadj=1, cfl=cfl)
+    return Problem("bryan2d", cfg, x1f, u, w,
+                   dict(tlim=1000.0, out_dt=100.0, p0=p0, qt=qt))
+
+
 def moist_profile(th, z, Ts=300.0, Ttop=200.0, ps=1.0e5, rh=0.8, zmoist=10.0e3,
                   nsub=16):
     """Horizontally uniform moist column at heights z (cell centres):

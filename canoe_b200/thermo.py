@@ -164,3 +164,58 @@ def svp(th, v, T, phase="auto"):
     beta = np.where(liquid, th.beta_l[v], th.beta_s[v])
     delta = np.where(liquid, th.delta_l[v], th.delta_s[v])
     return p3 * np.exp(beta * (1.0 - t3 / T) - delta * np.log(T / t3))
+
+
+# ---------------------------------------------------------------------------
+# saturated equilibrium of one condensable family (vapour slot 1, liquid slot
+# 2, no ice), host side, for the moist problem generators
+
+def sat_split(th, T, p, qt, v=0):
+    """Vapour and liquid mass fractions of a parcel with total water mass
+    fraction qt in equilibrium at (T, p): the vapour pressure at saturation
+    where water condenses, all vapour below it.  With rho q_v R_v T = e_s and
+    rho = p / (R_d f_eps T): q_v = (1 - q_t) e_s / ((1 + imr) (p - e_s))."""
+    phase = "liquid" if th.ice_slot[v] < 0 else "auto"
+    es = svp(th, v, np.asarray(T, dtype=np.float64), phase)
+    imr = th.inv_mu_ratio_m1[v]
+    qs = (1.0 - qt) * es / ((1.0 + imr) * (p - es))
+    qv = np.minimum(qs, qt)
+    return qv, qt - qv
+
+
+def enthalpy(th, q, T):
+    """Specific enthalpy e + p / rho of the mixture with mass fractions q
+    (slots 1..ny): e = c_v,d (q_d + sum q_n (1 + cv_ratio_m1)) T + sum q_n u0_n,
+    p / rho = R_d f_eps T (the energy of prim_to_cons per unit mass)."""
+    cvd = th.rd / (th.gammad - 1.0)
+    qsum = sum(q[n] for n in range(th.ny))
+    cvs = 1.0 - qsum
+    lat = 0.0
+    for n in range(th.ny):
+        cvs = cvs + q[n] * (1.0 + th.cv_ratio_m1[n])
+        lat = lat + q[n] * th.u0[n]
+    return cvd * cvs * T + lat + th.rd * feps_of(th, q) * T
+
+
+def theta_e(th, q, T, p, p0=1.0e5, v=0):
+    """Equivalent potential temperature, Emanuel (1994) eq. 4.5.11 in the
+    reference's form (src/snap/thermodynamics/atm_thermodynamics.hpp:43-98):
+    T (p0 / p_d)^(R_d q_d / c_pt) rh^(-R_v q_v / c_pt) exp(L_v q_v / (c_pt T)),
+    c_pt = c_pd q_d + c_l q_t, with this thermo's latent heat
+    L_v = R_v (beta_l t3 - delta_l T) and liquid c_l."""
+    qv = q[v]
+    ql = q[th.liq_slot[v] - 1]
+    qd = 1.0 - sum(q[n] for n in range(th.ny))
+    cvd = th.rd / (th.gammad - 1.0)
+    cpd = th.rd + cvd
+    rv = th.rd * (1.0 + th.inv_mu_ratio_m1[v])
+    cl = cvd * (1.0 + th.cv_ratio_m1[th.liq_slot[v] - 1])
+    lv = rv * (th.beta_l[v] * th.t3[v] - th.delta_l[v] * T)
+    xd, xv = qd / th.rd, qv / rv  # moles per unit mass times R
+    pd = xd / (xd + xv) * p
+    e = xv / (xd + xv) * p
+    phase = "liquid" if th.ice_slot[v] < 0 else "auto"
+    rh = e / svp(th, v, np.asarray(T, dtype=np.float64), phase)
+    cpt = cpd * qd + cl * (qv + ql)
+    return (T * (p0 / pd) ** (th.rd * qd / cpt) * rh ** (-rv * qv / cpt)
+            * np.exp(lv * qv / (cpt * T)))

@@ -1,4 +1,7 @@
-"""The rising-bubble regression run on the GPU: robert2d.inp's configuration
+"""The regression runs of the reference's examples on the GPU: the dry
+rising bubble of robert2d.inp and the moist bubble of bryan.inp (below).
+
+The dry run: robert2d.inp's configuration
 (canoe_b200.problems.robert2d, 300 x 200 cells to tlim = 1080 s, about
 170 k cycles) stepped by the CUDA library through the main loop
 (canoe_b200.driver.evolve), written every 180 s by the NetCDF writer and
@@ -105,3 +108,52 @@ def test_mesh_outputs_equal_the_single_block_outputs(tmp_path):
                                   output.read_variable(pb, name)), name
     m.close()
     one.close()
+
+
+# ---------------------------------------------------------------------------
+# The moist rising bubble (bryan.inp, canoe_b200.problems.bryan2d: 200 x 400
+# cells to 1000 s, about 15 k cycles, the saturation adjustment condensing
+# and evaporating up to 1 g/kg), written every 100 s and held by the check of
+# examples/2019-Li-snap/test_bryan.py (theta_e[3, 0, :, :], the bottom row at
+# the fourth output, below 900) and over the whole field.  This flow is far
+# less sensitive to roundoff: a twin run differs by a theta_e L2 norm of
+# 1.1e-3 K at 300 s and 2.9e-3 K at 1000 s (against an anomaly norm of about
+# 100 K), and the CUDA path differs from the oracle by 1.1e-3 and 3.1e-3 K.
+
+B300 = os.path.join(GOLD, "bryan2d_ppm.theta_e.00000-00300s.nc")
+B1000 = os.path.join(GOLD, "bryan2d_ppm.theta_e.01000s.nc")
+
+
+def _bryan(p, tmp_path, name):
+    blk = MeshBlock(p)
+    out = output.NetcdfOutput(str(tmp_path / name), dt=p.meta["out_dt"], p0=p.meta["p0"],
+                              variables=("theta_e",))
+    t, cycles = driver.evolve(blk, p.meta["tlim"], [out])
+    assert blk.error_word() == 0
+    blk.close()
+    assert t == p.meta["tlim"] and len(out.written) == 11
+    joined = output.join_records(out.written[:4], str(tmp_path / f"{name}.joined.nc"))
+    return joined, out.written[-1], cycles
+
+
+def _field_l2(a, rec_a, b, rec_b):
+    x = output.read_variable(a, "theta_e")[rec_a].astype(np.float64)
+    y = output.read_variable(b, "theta_e")[rec_b].astype(np.float64)
+    return float(np.sqrt(((x - y) ** 2).sum()))
+
+
+@pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "fp32"])
+def test_bryan2d_matches_the_oracle_run(tmp_path, mixed):
+    p = problems.bryan2d()
+    if mixed:
+        p.cfg.precision = FP32_PERTURBATION
+    joined, last, cycles = _bryan(p, tmp_path, "bryan")
+    d_ref = output.check("bryan", joined, B300)
+    d300 = _field_l2(joined, 3, B300, 3)
+    d1000 = _field_l2(last, -1, B1000, -1)
+    print(f"bryan2d {'FP32 perturbation' if mixed else 'FP64'}: {cycles} cycles, theta_e L2 vs "
+          f"oracle {d_ref:.2e} K (bottom row at 300 s), {d300:.2e} K at 300 s, "
+          f"{d1000:.2e} K at 1000 s")
+    bar = 2.0 if mixed else 1.0
+    assert d300 < bar * 5e-3
+    assert d1000 < bar * 1e-2

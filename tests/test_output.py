@@ -211,3 +211,57 @@ def test_golden_of_the_robert_run(t, name, zmin):
     # the warm anomaly's centre of mass has risen above z = 260 m
     zc = float((z[:, None] * (th - 303.15) * warm).sum() / ((th - 303.15) * warm).sum())
     assert zc > zmin
+
+
+def test_bryan_initial_state():
+    """bryan2d: a saturated reversible moist adiabat (theta_e nearly
+    constant up the column, liquid everywhere, total water qt) and the
+    virtual-temperature bubble of bryan.cpp:125-155 at constant pressure."""
+    from canoe_b200 import thermo as T
+    p = problems.bryan2d(nx1=50, nx2=100)
+    th = p.cfg.thermo
+    w = p.interior(p.w)[:, 0]  # (n, j, i)
+    q = w[1:3]
+    assert np.allclose(q[0] + q[1], 0.0196, rtol=0, atol=1e-12)
+    assert (q[1] > 0).all()
+    temp = w[4 + th.ny] / (w[0] * th.rd * T.feps_of(th, q))
+    te = T.theta_e(th, q, temp, w[4 + th.ny])
+    far = te[0]  # the column at x = 100 m, far from the bubble
+    assert 319.0 < far.min() and far.max() < 322.0 and far.max() - far.min() < 1.0
+    # saturated: the vapour sits at saturation in every cell
+    qv, _ = T.sat_split(th, temp, w[4 + th.ny], 0.0196)
+    np.testing.assert_allclose(q[0], qv, rtol=1e-9)
+    # the bubble: T_v raised by dT cos^2(pi L / 2) T_v / 300 at its centre
+    j, i = 50, 9  # x = 10.1 km, z = 1.9 km: L = 0.07
+    tv, tv0 = temp[j, i] * T.feps_of(th, q[:, j, i]), temp[0, i] * T.feps_of(th, q[:, 0, i])
+    L = np.hypot((10.1e3 - 10.0e3) / 2.0e3, (1.9e3 - 2.0e3) / 2.0e3)
+    assert abs(tv / tv0 - (1 + 2.0 * np.cos(np.pi * L / 2) ** 2 / 300.0)) < 1e-9
+
+
+def test_join_records_and_the_bryan_check(tmp_path):
+    p = problems.bryan2d(nx1=20, nx2=40)
+    o = output.NetcdfOutput(str(tmp_path / "b"), dt=1.0, variables=("theta_e",))
+    for t in range(4):
+        o.write(_Block(p, p.w), float(t))
+    j = output.join_records(o.written, str(tmp_path / "j.nc"))
+    assert list(output.read_variable(j, "time")) == [0.0, 1.0, 2.0, 3.0]
+    te = output.read_variable(j, "theta_e")
+    assert te.shape == (4, 20, 40, 1)
+    assert output.check("bryan", j, j) == 0.0
+
+
+@pytest.mark.parametrize("name,nrec,t", [("00000-00300s", 4, 300.0), ("01000s", 1, 1000.0)])
+def test_golden_of_the_bryan_run(name, nrec, t):
+    """The committed oracle outputs of the bryan2d run
+    (tests/golden/make_bryan_golden.py): theta_e only, the bubble's theta_e
+    above the environment's at the same height, and risen by 1000 s."""
+    path = os.path.join(os.path.dirname(GOLDEN), f"bryan2d_ppm.theta_e.{name}.nc")
+    with netcdf_file(path, "r", mmap=False) as f:
+        assert f.variables["theta_e"].shape == (nrec, 200, 400, 1)
+        assert abs(float(f.variables["time"][-1]) - t) < 0.1
+        te = f.variables["theta_e"][-1, :, :, 0].astype(np.float64)
+    assert 319.0 < te.min() and te.max() < 323.5
+    anomaly = te - te[:, :20].mean(axis=1)[:, None]  # against the far columns
+    assert anomaly.max() > 1.0
+    zmax = np.unravel_index(np.argmax(anomaly), anomaly.shape)[0]
+    assert zmax > (60 if t > 500 else 30)  # the bubble started at index 38-40
