@@ -85,6 +85,7 @@ SIGNATURES = [
     ("canoe_block_use_graph", c_int, [c_void_p, c_int]),
     ("canoe_block_synchronize", c_int, [c_void_p]),
     ("canoe_block_set_fixed_dt", c_int, [c_void_p, c_double]),
+    ("canoe_block_set_diffusion", c_int, [c_void_p, c_double, c_double]),
     ("canoe_block_step_profile", c_int, [c_void_p, c_double, POINTER(ctypes.c_float), c_int]),
     ("canoe_block_step", c_int, [c_void_p, c_double]),
     ("canoe_block_step_noalloc", c_int, [POINTER(BlockConfig), c_void_p, c_void_p, c_void_p,

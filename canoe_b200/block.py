@@ -74,6 +74,10 @@ class MeshBlock:
         check(self.lib.canoe_block_satadj_stats(self.h, s.ctypes.data), "satadj_stats")
         return s
 
+    def set_diffusion(self, K, p0=1.0e5):
+        """the dense sinking bubble's dissipation source (straka.cpp:125-190)"""
+        check(self.lib.canoe_block_set_diffusion(self.h, float(K), float(p0)), "set_diffusion")
+
     def set_fixed_dt(self, dt):
         check(self.lib.canoe_block_set_fixed_dt(self.h, float(dt)), "set_fixed_dt")
 

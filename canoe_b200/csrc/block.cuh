@@ -130,6 +130,11 @@ struct SlabSet {
 };
 int launch_exchange(const SlabSet &ss, cudaStream_t st);
 
+// the dissipation source of the dense sinking bubble (source.cu): du +=
+// beta dt K rho / (dx dy) (lap v1, lap v2, cp T / theta lap theta), 2-D
+int launch_diffusion(const Geom &g, const canoe_thermo_t &th, const double *w, double *du,
+                     const double *dtp, double beta, double K, double p0, cudaStream_t st);
+
 // all checks a block configuration passes before a step runs on it (capi.cu);
 // 0 or a canoe_status with the message set
 int validate_block_config(const canoe_block_config_t &c);

@@ -153,6 +153,8 @@ struct canoe_block {
   // w that canoe_block_exchange_ghosts copies from the neighbours
   canoe_block *nb[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   SlabSet slabs{};
+  // user source: the sinking bubble's dissipation (diffusivity, p0; 0 = off)
+  double diff_K = 0., diff_p0 = 1.e5;
 };
 
 // Every check a block configuration must pass before a step may run on it
@@ -286,6 +288,10 @@ static int stage_launches(canoe_block *b, int s, double *dtp, unsigned long long
                                     b->d_w, b->d_du, dtp, sg.beta, nullptr, st)))
     return rc;
   CB_MARK(2);
+  // user sources into du (AddSourceTerms), before the x1 pencil solves it
+  if (b->diff_K > 0. &&
+      (rc = launch_diffusion(g, b->th, b->d_w, b->d_du, dtp, sg.beta, b->diff_K, b->diff_p0, st)))
+    return rc;
   if (!b->lines) {
     if ((rc = launch_x1col(g, b->th, b->cfg.recon, b->cfg.rsolver, b->cfg.implicit_flag,
                            b->cfg.precision, kColStep, b->d_w, b->d_du, b->d_u, b->d_u1, dtp,
@@ -596,6 +602,24 @@ int canoe_block_solve_implicit(canoe_block_t b, double *d_du, double dt) {
 int canoe_block_use_graph(canoe_block_t b, int on) {
   if (!b) return CANOE_ERR_ARG;
   b->graph = on != 0;
+  return 0;
+}
+
+int canoe_block_set_diffusion(canoe_block_t b, double K, double p0) {
+  if (!b || !(K >= 0.) || !(p0 > 0.)) {
+    set_error("diffusivity must be >= 0 and p0 > 0");
+    return CANOE_ERR_ARG;
+  }
+  if (K > 0. && (b->g.nx3 != 1 || b->g.nx2 < 2 || b->lines)) {
+    set_error("the dissipation source is defined on 2-D blocks without x2 implicit solves");
+    return CANOE_ERR_UNSUPPORTED;
+  }
+  b->diff_K = K;
+  b->diff_p0 = p0;
+  if (b->gexec) {  // the captured step changes
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
   return 0;
 }
 

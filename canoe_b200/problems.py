@@ -140,6 +140,41 @@ def robert2d(nx1=300, nx2=200, recon=RECON_PPM):
     return p
 
 
+def straka2d(nx1=64, nx2=256, x1max=6.4e3, x2max=25.6e3, Ts=300.0, p0=1.0e5, dT=-15.0,
+             xc=0.0, xr=4.0e3, zc=3.0e3, zr=2.0e3, grav=9.8, K=75.0, cfl=0.45,
+             recon=RECON_PPM, rsolver=RS_LMARS):
+    """The dense sinking bubble of examples/2019-Li-snap/straka.inp /
+    straka.cpp:219-262 (Straka et al. 1993): a dry adiabat from Ts, a cold
+    bubble of dT (cos(pi L) + 1) / 2 for L <= 1 centred on the left wall,
+    reflecting walls; the dissipation source of diffusivity K (straka.cpp:
+    125-190) is turned on by the caller with set_diffusion(meta["K"],
+    meta["p0"]).  Courant number 0.9 split over the two directions as in
+    bubble2d; fifth-order horizontal reconstruction replaced by PPM."""
+    th = T.dry(gammad=1.4, grav=-grav)
+    Rd = th.rd
+    cp = 1.4 / 0.4 * Rd
+    x1f = np.linspace(0.0, x1max, nx1 + 1)
+    z = 0.5 * (x1f[1:] + x1f[:-1])
+    dx2 = x2max / nx2
+    x2v = (np.arange(nx2) + 0.5) * dx2
+    zz, xx = np.meshgrid(z, x2v)  # (j, i)
+    L = np.sqrt(((xx - xc) / xr) ** 2 + ((zz - zc) / zr) ** 2)
+    temp = Ts - grav * zz / cp
+    pres = p0 * (temp / Ts) ** (cp / Rd)
+    temp = np.where(L <= 1.0, temp + dT * (np.cos(np.pi * L) + 1.0) / 2.0, temp)
+    nv = 5
+    w_int = np.zeros((nv, 1, nx2, nx1))
+    w_int[0, 0] = pres / (Rd * temp)
+    w_int[4, 0] = pres
+    shape = _shape(nx1, nx2, 1, nv)
+    w = _embed(shape, w_int, nx1, nx2, 1)
+    u = _embed(shape, T.prim_to_cons(th, w_int), nx1, nx2, 1)
+    bc = [BC_REFLECT] * 4 + [BC_PERIODIC] * 2
+    cfg, x1f = make_config(nx1, nx2, 1, x1f, dx2, 1.0, th, bc, recon, rsolver,
+                           implicit_flag=0, satadj=0, cfl=cfl)
+    return Problem("straka2d", cfg, x1f, u, w, dict(tlim=900.0, out_dt=300.0, p0=p0, K=K))
+
+
 def _solve_T(f, lo, hi, it=60):
     """Bisection of the increasing function f on [lo, hi] (arrays)."""
     lo, hi = np.array(lo, dtype=np.float64), np.array(hi, dtype=np.float64)

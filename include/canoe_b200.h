@@ -337,6 +337,16 @@ int canoe_block_step_profile(canoe_block_t b, double dt, float *ms, int nclass);
  * (Athena <time> dt); no direct counterpart. */
 int canoe_block_set_fixed_dt(canoe_block_t b, double dt);
 
+/* User explicit source of the stage: the viscous and thermal dissipation
+ * of the dense sinking bubble example with diffusivity K [m^2/s] and
+ * reference pressure p0 of its potential temperature, added into du with
+ * the stage weight before the implicit solve (the Diffusion function that
+ * examples/2019-Li-snap/straka.cpp:125-190 enrolls with
+ * EnrollUserExplicitSourceFunction, applied by
+ * ImplicitHydroTasks::AddSourceTerms, src/tasklist/implicit_hydro_tasks.cpp:
+ * 192-216).  2-D blocks (nx3 = 1) only; K = 0 turns it off. */
+int canoe_block_set_diffusion(canoe_block_t b, double K, double p0);
+
 /* wait for the block's stream (steps are asynchronous) */
 int canoe_block_synchronize(canoe_block_t b);
 

@@ -45,6 +45,11 @@ void oracle_block_set_roundtrip(void *h, int on) {
   static_cast<Block *>(h)->fix_roundtrip = on != 0;
 }
 
+void oracle_block_set_diffusion(void *h, double K, double p0) {
+  static_cast<Block *>(h)->diff_K = K;
+  static_cast<Block *>(h)->diff_p0 = p0;
+}
+
 int oracle_block_set_conserved(void *h, const double *u) {
   Block &b = *static_cast<Block *>(h);
   std::memcpy(b.u.data(), u, b.u.size() * sizeof(double));

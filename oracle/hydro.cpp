@@ -720,6 +720,43 @@ void add_gravity_source(Block &b, double dt, std::vector<double> &du) {
       }
 }
 
+// The user explicit source of the dense sinking bubble example:
+// examples/2019-Li-snap/straka.cpp:125-190 (Diffusion), 2-D (k = ks), added
+// into du with the stage weight as ImplicitHydroTasks::AddSourceTerms does
+// (src/tasklist/implicit_hydro_tasks.cpp:192-216).  dx = dx1f(is), dy =
+// dx2f(js); theta = T (p0 / p)^chi with T from the equation of state.
+void add_diffusion_source(Block &b, double dt, std::vector<double> &du) {
+  const double K = b.diff_K;
+  if (K <= 0.) return;
+  const double chi = (b.th.gammad - 1.) / b.th.gammad;
+  const double cp = b.th.gammad / (b.th.gammad - 1.) * b.th.rd;
+  const double dx = b.dx1f[b.is], dy = b.dx2;
+  const int64_t s = (int64_t)b.cells();
+  const int k = b.ks;
+  auto theta = [&](int j, int i, double &T) {
+    const double *w = &b.w[b.idx(0, k, j, i)];
+    T = temperature_of_prim(b.th, w, s);
+    return T * std::pow(b.diff_p0 / w[b.ipr * s], chi);
+  };
+#pragma omp parallel for schedule(static)
+  for (int j = b.js; j <= b.je; ++j)
+    for (int i = b.is; i <= b.ie; ++i) {
+      auto W = [&](int n, int jj, int ii) { return b.w[b.idx(n, k, jj, ii)]; };
+      double T, Tn;
+      const double th = theta(j, i, T);
+      const double th_sum = theta(j + 1, i, Tn) + theta(j - 1, i, Tn) + theta(j, i + 1, Tn) +
+                            theta(j, i - 1, Tn);
+      const double f = dt * K * W(0, j, i) / (dx * dy);
+      du[b.idx(b.ivx, k, j, i)] += f * (W(b.ivx, j, i - 1) + W(b.ivx, j, i + 1) +
+                                        W(b.ivx, j - 1, i) + W(b.ivx, j + 1, i) -
+                                        4. * W(b.ivx, j, i));
+      du[b.idx(b.ivy, k, j, i)] += f * (W(b.ivy, j, i - 1) + W(b.ivy, j, i + 1) +
+                                        W(b.ivy, j - 1, i) + W(b.ivy, j + 1, i) -
+                                        4. * W(b.ivy, j, i));
+      du[b.idx(b.ipr, k, j, i)] += f * cp * T / th * (th_sum - 4. * th);
+    }
+}
+
 // Hydro::NewBlockTimeStep with canoe patches/21.new_blockdt.patch:20-40
 // (an implicit direction uses |v| only: x1 when nx2 > 1, x2 and x3 by their
 // bits); returns cfl * min over interior cells.
@@ -774,6 +811,7 @@ void stage_step(Block &b, double dt, int stage) {
     double wght = be[stage] * dt;
     add_flux_divergence(b, wght, b.du);
     add_gravity_source(b, wght, b.du);
+    add_diffusion_source(b, wght, b.du);
     if (b.cfg.implicit_flag & 7) solve_implicit(b, b.du, wght);
 #pragma omp parallel for collapse(3) schedule(static)
     for (int n = 0; n < b.nv; ++n)

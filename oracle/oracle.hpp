@@ -57,6 +57,8 @@ struct Block {
   // decomposition scratch (canoe decomposition.hpp:77-87)
   std::vector<double> psf, psv, gam;  // (nc3,nc2,nc1+1), (nc3,nc2,nc1) x2
   bool fix_roundtrip = true;  // write the T/p' round trip back into w
+  // user source: the sinking bubble's dissipation (diffusivity, p0; 0 = off)
+  double diff_K = 0., diff_p0 = 1.e5;
   // cubed-sphere panel: geometry and blockID - 1 (nullptr / -1 otherwise)
   const ShellGeo *geo = nullptr;
   int panel = -1;

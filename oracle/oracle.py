@@ -36,6 +36,7 @@ def load():
         ("oracle_block_new", c_void_p, [POINTER(BlockConfig)]),
         ("oracle_block_free", None, [c_void_p]),
         ("oracle_block_set_roundtrip", None, [c_void_p, c_int]),
+        ("oracle_block_set_diffusion", None, [c_void_p, c_double, c_double]),
         ("oracle_block_set_conserved", c_int, [c_void_p, c_void_p]),
         ("oracle_block_set_primitive", c_int, [c_void_p, c_void_p]),
         ("oracle_block_get_conserved", c_int, [c_void_p, c_void_p]),
@@ -107,6 +108,9 @@ class OracleBlock:
         u = np.ascontiguousarray(u, dtype=np.float64)
         assert u.shape == self.shape
         self.lib.oracle_block_set_conserved(self.h, u.ctypes.data)
+
+    def set_diffusion(self, K, p0=1.0e5):
+        self.lib.oracle_block_set_diffusion(self.h, float(K), float(p0))
 
     def set_primitive(self, w):
         w = np.ascontiguousarray(w, dtype=np.float64)

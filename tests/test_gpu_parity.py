@@ -13,6 +13,7 @@ import pytest
 from canoe_b200 import MeshBlock, problems, thermo
 from canoe_b200._abi import (BC_REFLECT, RECON_PLM, RECON_PPM, RS_HLLC, RS_LMARS,
                              SatOpts, check, load)
+from canoe_b200._abi import CanoeError
 from conftest import max_var_rel_l2, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -181,6 +182,34 @@ def test_flux_runs_at_run_size(oracle_mod, fp32):
         gpu.step(dt)
         assert rel_l2(p.interior(gpu.conserved()), p.interior(ora.conserved())) < 1e-11
     gpu.close()
+
+
+def test_dissipation_source_steps(oracle_mod):
+    """The sinking bubble's user source (canoe_block_set_diffusion, straka.cpp:
+    125-190) on a small 2-D block: three steps against the oracle; a 3-D
+    block refuses it."""
+    p = perturb(problems.straka2d(nx1=32, nx2=64, x1max=3.2e3, x2max=6.4e3, xr=2.0e3,
+                                  zc=1.5e3, zr=1.0e3), dv=0.5)
+    gpu = MeshBlock(p)
+    gpu.set_diffusion(75.0)
+    ora = oracle_mod.OracleBlock(p)
+    ora.set_diffusion(75.0)
+    plain = oracle_mod.OracleBlock(p)
+    for _ in range(3):
+        dt = ora.new_dt()
+        ora.step(dt)
+        plain.step(dt)
+        gpu.step(dt)
+    a, b = p.interior(gpu.conserved()), p.interior(ora.conserved())
+    assert max_var_rel_l2(a, b) < 1e-11
+    # the source changes the state well above that bar
+    assert max_var_rel_l2(p.interior(plain.conserved()), b) > 1e-6
+    gpu.close()
+    q = small_c2()
+    g3 = MeshBlock(q)
+    with pytest.raises(CanoeError):
+        g3.set_diffusion(75.0)
+    g3.close()
 
 
 @pytest.mark.parametrize("case", ["c2_ppm_hllc", "c2_full5x5"])

@@ -265,3 +265,32 @@ def test_golden_of_the_bryan_run(name, nrec, t):
     assert anomaly.max() > 1.0
     zmax = np.unravel_index(np.argmax(anomaly), anomaly.shape)[0]
     assert zmax > (60 if t > 500 else 30)  # the bubble started at index 38-40
+
+
+@pytest.mark.parametrize("name,t", [("00300s", 300.0), ("00900s", 900.0)])
+def test_golden_of_the_straka_run(name, t):
+    """The committed oracle outputs of the straka2d run
+    (tests/golden/make_straka_golden.py): the cold front moving right along
+    the ground, at about 15 km by 900 s (Straka et al. 1993 report 14.4 to
+    15.5 km across their resolutions)."""
+    path = os.path.join(os.path.dirname(GOLDEN), f"straka2d_ppm.theta.{name}.nc")
+    with netcdf_file(path, "r", mmap=False) as f:
+        assert abs(float(f.variables["time"][0]) - t) < 0.2
+        th = f.variables["theta"][0, :, :, 0].astype(np.float64)  # (x1, x2)
+        x2 = f.variables["x2"][:].astype(np.float64)
+    assert th.shape == (64, 256)
+    assert 285.0 < th.min() < 295.0 and th.max() < 300.5
+    front = x2[np.where((th < 299.0).any(axis=0))[0].max()]
+    assert (3.5e3 < front < 6.0e3) if t < 500 else (14.0e3 < front < 16.0e3)
+
+
+def test_straka_initial_state():
+    """straka.cpp:219-262: the dry adiabat (theta = Ts away from the bubble)
+    and the cold bubble, -15 K in temperature (-16.6 K in theta at 3 km) at
+    its centre on the left wall."""
+    p = problems.straka2d()
+    f = output.cell_fields(p.cfg, p.w, ("uov",), p.meta["p0"])
+    th = f["theta"][:, :, 0]  # (x1, x2)
+    assert np.allclose(th[:, -1], 300.0, rtol=0, atol=1e-9)
+    i = 29  # z = 2950 m, x = 50 m: L = 0.027
+    assert -17.0 < th[i, 0] - 300.0 < -16.0
