@@ -22,6 +22,16 @@ struct Slots {
                        NV = 5 + NY;
 };
 
+// Division in the FP32 perturbation solvers: the fast reciprocal-based
+// __fdividef (2 ulp) for R = float, exact for R = double.  The FP32 path's
+// stated error (relative 1e-5 on fluxes) is far above it.
+constexpr bool kFastDiv = true;
+template <typename R>
+__device__ __forceinline__ R pdiv(R a, R b) {
+  if constexpr (sizeof(R) == 4 && kFastDiv) return __fdividef(a, b);
+  else return a / b;
+}
+
 // Mixture adiabatic index from mass fractions w[1..NY]
 // (canoe src/interface/eos.hpp:48-67, rho = 1).
 template <typename R, int NY>
@@ -306,17 +316,17 @@ __device__ __forceinline__ void lmars_pert(const canoe_thermo_t &th, const R *wl
   constexpr int ivz = S::IVX + (DIR + 2) % 3;
   constexpr int ipr = S::IPR;
   const R pl = pref + wli[ipr], pr = pref + wri[ipr];
-  R kappal = R(1) / (get_gamma<R, NY>(th, wli) - R(1));
-  R kappar = R(1) / (get_gamma<R, NY>(th, wri) - R(1));
-  R hl = pl / wli[0] * (kappal + R(1)) +
+  R kappal = pdiv(R(1), get_gamma<R, NY>(th, wli) - R(1));
+  R kappar = pdiv(R(1), get_gamma<R, NY>(th, wri) - R(1));
+  R hl = pdiv(pl, wli[0]) * (kappal + R(1)) +
          R(0.5) * (wli[ivx] * wli[ivx] + wli[ivy] * wli[ivy] + wli[ivz] * wli[ivz]);
-  R hr = pr / wri[0] * (kappar + R(1)) +
+  R hr = pdiv(pr, wri[0]) * (kappar + R(1)) +
          R(0.5) * (wri[ivx] * wri[ivx] + wri[ivy] * wri[ivy] + wri[ivz] * wri[ivz]);
   R rhobar = R(0.5) * (wli[0] + wri[0]);
-  R cbar = sqrt(R(0.5) * (R(1) + (R(1) / kappar + R(1) / kappal) / R(2)) * (pl + pr) / rhobar);
+  R cbar = sqrt(pdiv(R(0.5) * (R(1) + (pdiv(R(1), kappar) + pdiv(R(1), kappal)) / R(2)) * (pl + pr), rhobar));
   // pbar - pref and ubar from pressure differences only
   R pbar = R(0.5) * (wli[ipr] + wri[ipr]) + R(0.5) * (rhobar * cbar) * (wli[ivx] - wri[ivx]);
-  R ubar = R(0.5) * (wli[ivx] + wri[ivx]) + R(0.5) / (rhobar * cbar) * (wli[ipr] - wri[ipr]);
+  R ubar = R(0.5) * (wli[ivx] + wri[ivx]) + pdiv(R(0.5), rhobar * cbar) * (wli[ipr] - wri[ipr]);
   R rdl = R(1), rdr = R(1);
 #pragma unroll
   for (int n = 1; n <= NY; ++n) {
@@ -365,11 +375,11 @@ __device__ __forceinline__ void hllc_pert(const canoe_thermo_t &th, const R *wl,
   const R dpl = wl[IPR], dpr = wr[IPR];     // p' on each side
   const R pl = pref + dpl, pr = pref + dpr;  // absolute, for relative uses
   R gammal = get_gamma<R, NY>(th, wli);
-  R kappal = R(1) / (gammal - R(1));
+  R kappal = pdiv(R(1), gammal - R(1));
   R gammar = get_gamma<R, NY>(th, wri);
-  R kappar = R(1) / (gammar - R(1));
-  R cl = sqrt(gammal * pl / wli[0]);
-  R cr = sqrt(gammar * pr / wri[0]);
+  R kappar = pdiv(R(1), gammar - R(1));
+  R cl = sqrt(pdiv(gammal * pl, wli[0]));
+  R cr = sqrt(pdiv(gammar * pr, wri[0]));
   R KE_l, KE_r;
   if constexpr (COVKE) {
     R vy = wli[IVY] + wli[IVZ] * ke_cth, vz = wli[IVZ] + wli[IVY] * ke_cth;
@@ -387,8 +397,8 @@ __device__ __forceinline__ void hllc_pert(const canoe_thermo_t &th, const R *wl,
   R ca = R(.5) * (cl + cr);
   R dpmid = R(.5) * (dpl + dpr + (wli[IVX] - wri[IVX]) * rhoa * ca);
   R pmid = pref + dpmid;
-  R ql = (dpmid <= dpl) ? R(1) : sqrt(R(1) + (gammal + R(1)) / (R(2) * gammal) * (pmid / pl - R(1)));
-  R qr = (dpmid <= dpr) ? R(1) : sqrt(R(1) + (gammar + R(1)) / (R(2) * gammar) * (pmid / pr - R(1)));
+  R ql = (dpmid <= dpl) ? R(1) : sqrt(R(1) + pdiv(gammal + R(1), R(2) * gammal) * (pdiv(pmid, pl) - R(1)));
+  R qr = (dpmid <= dpr) ? R(1) : sqrt(R(1) + pdiv(gammar + R(1), R(2) * gammar) * (pdiv(pmid, pr) - R(1)));
   R al = wli[IVX] - cl * ql;
   R ar = wri[IVX] + cr * qr;
   R bp = ar > R(0) ? ar : R(TINY_NUMBER);
@@ -399,8 +409,8 @@ __device__ __forceinline__ void hllc_pert(const canoe_thermo_t &th, const R *wl,
   R tr = dpr + vxr * wri[0] * wri[IVX];
   R ml = wli[0] * vxl;
   R mr = -(wri[0] * vxr);
-  R am = (tl - tr) / (ml + mr);
-  R dcp = (ml * tr + mr * tl) / (ml + mr);  // contact pressure minus pref
+  R am = pdiv(tl - tr, ml + mr);
+  R dcp = pdiv(ml * tr + mr * tl, ml + mr);  // contact pressure minus pref
   dcp = dcp > -pref ? dcp : -pref;
   vxl = wli[IVX] - bm;
   vxr = wri[IVX] - bp;
@@ -412,13 +422,13 @@ __device__ __forceinline__ void hllc_pert(const canoe_thermo_t &th, const R *wl,
   }
   R sl, sr, sm;
   if (am >= R(0)) {
-    sl = am / (am - bm);
+    sl = pdiv(am, am - bm);
     sr = R(0);
-    sm = -bm / (am - bm);
+    sm = pdiv(-bm, am - bm);
   } else {
     sl = R(0);
-    sr = -am / (bp - am);
-    sm = bp / (bp - am);
+    sr = pdiv(-am, bp - am);
+    sm = pdiv(bp, bp - am);
   }
   R f[S::NV];
   f[0] = sl * (wli[0] * vxl * rdl) + sr * (wri[0] * vxr * rdr);
