@@ -196,8 +196,8 @@ __device__ __forceinline__ void jacobian(M<N> &d, double gm1_, const double *w) 
   T v1 = T(w[S::IVX]), v2 = T(w[S::IVY]), v3 = T(w[S::IVZ]);
   T rho = T(w[0]), pres = T(w[S::IPR]);
   T s2 = v1 * v1 + v2 * v2 + v3 * v3;
-  T c1 = ((gm1 - T(1)) * s2 / T(2) - (gm1 + T(1)) / gm1 * pres / rho) * v1;
-  T c2 = (gm1 + T(1)) / gm1 * pres / rho + s2 / T(2) - gm1 * v1 * v1;
+  T c1 = ((gm1 - T(1)) * s2 / T(2) - pdiv(pdiv(gm1 + T(1), gm1) * pres, rho)) * v1;
+  T c2 = pdiv(pdiv(gm1 + T(1), gm1) * pres, rho) + s2 / T(2) - gm1 * v1 * v1;
   const T f[5][5] = {{T(0), T(1), T(0), T(0), T(0)},
                      {gm1 * s2 / T(2) - v1 * v1, (T(2) - gm1) * v1, -gm1 * v2, -gm1 * v3, gm1},
                      {-v1 * v2, v2, v1, T(0), T(0)},
@@ -226,27 +226,28 @@ __device__ __forceinline__ void abs_jacobian(M<N> &A, const canoe_thermo_t &th,
   }
   T sqrtdl = sqrt(wl[0]);
   T sqrtdr = sqrt(wr[0]);
-  T isdlpdr = T(1) / (sqrtdl + sqrtdr);
+  T isdlpdr = pdiv(T(1), sqrtdl + sqrtdr);
   prim[0] = sqrtdl * sqrtdr;
   prim[S::IVX] = (sqrtdl * wl[S::IVX] + sqrtdr * wr[S::IVX]) * isdlpdr;
   prim[S::IVY] = (sqrtdl * wl[S::IVY] + sqrtdr * wr[S::IVY]) * isdlpdr;
   prim[S::IVZ] = (sqrtdl * wl[S::IVZ] + sqrtdr * wr[S::IVZ]) * isdlpdr;
 #pragma unroll
   for (int n = 1; n <= NY; ++n) prim[n] = (sqrtdl * wl[n] + sqrtdr * wr[n]) * isdlpdr;
-  T el = wl[S::IPR] / gm1 + T(0.5) * wl[0] *
+  T el = pdiv(wl[S::IPR], gm1) + T(0.5) * wl[0] *
          (wl[S::IVX] * wl[S::IVX] + wl[S::IVY] * wl[S::IVY] + wl[S::IVZ] * wl[S::IVZ]);
-  T er = wr[S::IPR] / gm1 + T(0.5) * wr[0] *
+  T er = pdiv(wr[S::IPR], gm1) + T(0.5) * wr[0] *
          (wr[S::IVX] * wr[S::IVX] + wr[S::IVY] * wr[S::IVY] + wr[S::IVZ] * wr[S::IVZ]);
-  T hbar = ((el + wl[S::IPR]) / sqrtdl + (er + wr[S::IPR]) / sqrtdr) * isdlpdr;
-  prim[S::IPR] = (hbar - T(0.5) * (prim[S::IVX] * prim[S::IVX] + prim[S::IVY] * prim[S::IVY] +
-                                   prim[S::IVZ] * prim[S::IVZ])) *
-                 gm1 / (gm1 + T(1)) * prim[0];
+  T hbar = (pdiv(el + wl[S::IPR], sqrtdl) + pdiv(er + wr[S::IPR], sqrtdr)) * isdlpdr;
+  prim[S::IPR] = pdiv((hbar - T(0.5) * (prim[S::IVX] * prim[S::IVX] +
+                                        prim[S::IVY] * prim[S::IVY] +
+                                        prim[S::IVZ] * prim[S::IVZ])) * gm1,
+                      gm1 + T(1)) * prim[0];
   T cs = sound_speed<T, NY>(th, prim);
   T r = prim[0], u = prim[S::IVX], v = prim[S::IVY], w = prim[S::IVZ], p = prim[S::IPR];
   T ke = T(0.5) * (u * u + v * v + w * w);
-  T hp = (gm1 + T(1)) / gm1 * p / r;
+  T hp = pdiv(pdiv(gm1 + T(1), gm1) * p, r);
   T h = hp + ke;
-  const T ihp = T(1) / hp, i2hp = T(0.5) * ihp, i2chp = i2hp / cs;
+  const T ihp = pdiv(T(1), hp), i2hp = T(0.5) * ihp, i2chp = pdiv(i2hp, cs);
   const T R[5][5] = {{T(1), T(1), T(1), T(0), T(0)},
                      {u - cs, u, u + cs, T(0), T(0)},
                      {v, v, v, T(1), T(0)},
