@@ -112,7 +112,8 @@ int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o,
                   double *u, int64_t ncells, int64_t stride, const Geom *g,
                   const double *t_guess, double *t_out, int32_t *iters,
                   unsigned long long *stats, cudaStream_t st,
-                  const MlpView *mlp = nullptr, double *guess_out = nullptr);
+                  const MlpView *mlp = nullptr, double *guess_out = nullptr,
+                  uint32_t *err = nullptr);
 MlpView mlp_view(const struct canoe_mlp *m);
 
 // ghost slabs copied between neighbouring blocks (exchange.cu): NV x nk x

@@ -322,7 +322,7 @@ static int stage_launches(canoe_block *b, int s, double *dtp, unsigned long long
     MlpView mv;
     if (b->mlp) mv = mlp_view(b->mlp);
     if ((rc = launch_satadj(b->th, o, b->d_u, nin, g.sv, &g, nullptr, nullptr, nullptr,
-                            b->d_sat, st, b->mlp ? &mv : nullptr, nullptr)))
+                            b->d_sat, st, b->mlp ? &mv : nullptr, nullptr, b->d_err)))
       return rc;
     CB_MARK(4);
   }

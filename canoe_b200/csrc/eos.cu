@@ -14,6 +14,8 @@
 //   cpp:290-313), Newton on T with a bracketed fallback.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "block.cuh"
 #include "mlp.cuh"
 
@@ -476,30 +478,38 @@ __device__ __forceinline__ bool may_condense(const canoe_thermo_t &th, const dou
   return any;
 }
 
+// the tensor-core state a CTA of the learned kernel carries across chunks
+struct UmmaState {
+  uint32_t phase;  // mbarrier phase of the next inference
+  bool live;       // false once a bounded wait gave up: no further inference
+  bool pending;    // the last inference's MMAs were not seen to complete
+};
+
 // The network's inference as a call rather than inlined code: most warps of
 // a step never run it (no cell near saturation), and inlined it would hold
-// registers across the Newton iteration of every warp (C2 learned
-// adjustment 0.733 -> 0.711 ms per step).
-__device__ __noinline__ float mlp_infer_call(const float *x, const float *sw1, const float *sb1,
-                                             const __nv_bfloat16 *sw2, const float *sb2,
-                                             const float *sw3, float b3) {
-  return mlp_warp_infer(x, sw1, sb1, sw2, sb2, sw3, b3);
+// registers across the Newton iteration of every warp.
+constexpr int kSatWg = 6;  // warpgroups per CTA of the learned adjustment (24 warps)
+
+__device__ __noinline__ float mlp_infer_call(uint8_t *sm, const float *p, const float *x,
+                                             bool warp_run, uint32_t phase, bool *ok) {
+  return mlp_umma_infer<kSatWg>(sm, p, x, warp_run, phase, ok);
 }
 
+// One chunk of the adjustment: this thread takes cell t.  With LEARNED the
+// chunk is the work of warpgroup wg, all of whose threads take part (it
+// holds the warpgroup's named barriers), and sm / us are the CTA's shared
+// memory and the warpgroup's tensor-core state.
 template <int NY, bool LEARNED>
-__global__ void __launch_bounds__(256, 3)
-    k_satadj(canoe_thermo_t th, canoe_satadj_opts_t o, double *__restrict__ u,
-             int64_t ncells, int64_t stride, Geom g, int use_geom,
-             const double *__restrict__ t_guess, double *__restrict__ t_out,
-             int32_t *__restrict__ iters, unsigned long long *stats, MlpView mv,
-             double *__restrict__ guess_out) {
+__device__ __forceinline__ void satadj_chunk(
+    const canoe_thermo_t &th, const canoe_satadj_opts_t &o, double *__restrict__ u,
+    int64_t ncells, int64_t stride, const Geom &g, int use_geom,
+    const double *__restrict__ t_guess, double *__restrict__ t_out,
+    int32_t *__restrict__ iters, unsigned long long *stats, const MlpView &mv,
+    double *__restrict__ guess_out, uint32_t *err, int64_t t, uint8_t *sm, UmmaState &us,
+    int wg) {
   using S = Slots<NY>;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int it = 0, fl = 0;
   bool active = t < ncells;
-  __shared__ float sw1[LEARNED ? kMlpH * kMlpIn : 1], sb1[LEARNED ? kMlpH : 1],
-      sb2[LEARNED ? kMlpH : 1], sw3[LEARNED ? kMlpH : 1];
-  __shared__ __align__(16) __nv_bfloat16 sw2[LEARNED ? kMlpH * kMlpH : 2];
   int64_t off = t;
   double uc[S::NV];
   if (active) {
@@ -516,33 +526,33 @@ __global__ void __launch_bounds__(256, 3)
   double tdry = 0.;
   bool need = false;
   if constexpr (LEARNED) {
-    // every lane of the warp takes part in the tensor-core inference
-    // (a warp whose cells all stay unsaturated skips the inference)
+    // the chunk's cells go through the tensor cores together (tcgen05,
+    // mlp_umma_infer); a chunk with no cell near saturation skips the
+    // inference, and within one that runs it, so does a warp whose cells all
+    // stay unsaturated
     float x[kMlpIn] = {0.f, 0.f, 0.f, 0.f};
     if (active) {
       tdry = mlp_features<NY>(th, uc, x);
       need = may_condense<NY>(th, uc, tdry);
     }
     tg = __longlong_as_double(0x7ff8000000000000LL);  // no guess: cold start
-    // the network's weights go to shared memory only for a CTA that has a
-    // cell near saturation (every thread reaches this barrier)
-    const bool cta_need = __syncthreads_or(need);
-    if (cta_need) {
-      for (int q = threadIdx.x; q < kMlpH * kMlpIn; q += blockDim.x) sw1[q] = mv.p[kMlpOffW1 + q];
-      for (int q = threadIdx.x; q < kMlpH; q += blockDim.x) {
-        sb1[q] = mv.p[kMlpOffB1 + q];
-        sb2[q] = mv.p[kMlpOffB2 + q];
-        sw3[q] = mv.p[kMlpOffW3 + q];
-      }
-      for (int q = threadIdx.x; q < kMlpH * kMlpH; q += blockDim.x) sw2[q] = mv.w2h[q];
-      __syncthreads();
-    }
-    if (cta_need && __any_sync(0xffffffffu, need)) {
+    // every thread of the warpgroup reaches this barrier
+    const bool wg_need = bar_red_or(1 + wg, kUmmaM, need);
+    if (wg_need && us.live) {
+      const bool warp_run = __any_sync(0xffffffffu, need);
 #pragma unroll
       for (int q = 0; q < kMlpIn; ++q)
         x[q] = active ? (x[q] - mv.in_mean[q]) * mv.in_istd[q] : 0.f;
-      const float yn = mlp_infer_call(x, sw1, sb1, sw2, sb2, sw3, mv.p[kMlpOffB3]);
-      if (need) tg = tdry + (double)(yn * mv.out_std + mv.out_mean);
+      bool ok = false;
+      const float yn = mlp_infer_call(sm, mv.p, x, warp_run, us.phase, &ok);
+      if (ok) {
+        us.phase ^= 1u;
+      } else {
+        us.live = false;
+        us.pending = true;
+        if (threadIdx.x % kUmmaM == 0 && err) atomicOr(err, (uint32_t)CANOE_EBIT_TIMEOUT);
+      }
+      if (need && ok) tg = tdry + (double)(yn * mv.out_std + mv.out_mean);
     }
     if (guess_out && active) guess_out[t] = tg;
   }
@@ -582,6 +592,45 @@ __global__ void __launch_bounds__(256, 3)
       if (d) atomicAdd(&stats[3], d);
     }
   }
+}
+
+
+// the cold start: one 256-cell chunk per CTA, three CTAs per SM (80
+// registers)
+template <int NY>
+__global__ void __launch_bounds__(256, 3)
+    k_satadj(canoe_thermo_t th, canoe_satadj_opts_t o, double *__restrict__ u,
+             int64_t ncells, int64_t stride, Geom g, int use_geom,
+             const double *__restrict__ t_guess, double *__restrict__ t_out,
+             int32_t *__restrict__ iters, unsigned long long *stats) {
+  UmmaState us{0u, false, false};
+  satadj_chunk<NY, false>(th, o, u, ncells, stride, g, use_geom, t_guess, t_out, iters, stats,
+                          MlpView{}, nullptr, nullptr,
+                          (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nullptr, us, 0);
+}
+
+// the learned start: one persistent CTA of kSatWg warpgroups per SM (a
+// kernel holding TMEM instructions is resident at one CTA per SM, mlp.cuh).
+// The CTA stages the network and allocates its TMEM once; warpgroup g of CTA
+// b then takes the 128-cell chunks b kSatWg + g, b kSatWg + g + gridDim.x
+// kSatWg, ..., independently of the CTA's other warpgroups.
+template <int NY>
+__global__ void __launch_bounds__(kSatWg * kUmmaM, 1)
+    k_satadj_learned(canoe_thermo_t th, canoe_satadj_opts_t o, double *__restrict__ u,
+                     int64_t ncells, int64_t stride, Geom g, int use_geom,
+                     const double *__restrict__ t_guess, double *__restrict__ t_out,
+                     int32_t *__restrict__ iters, unsigned long long *stats, MlpView mv,
+                     double *__restrict__ guess_out, uint32_t *err) {
+  extern __shared__ __align__(1024) uint8_t dsm[];
+  mlp_umma_setup<kSatWg>(dsm, mv.p, mv.w2h);
+  UmmaState us{0u, true, false};
+  const int wg = threadIdx.x / kUmmaM;
+  const int64_t nchunk = (ncells + kUmmaM - 1) / kUmmaM;
+  for (int64_t c = (int64_t)blockIdx.x * kSatWg + wg; c < nchunk;
+       c += (int64_t)gridDim.x * kSatWg)
+    satadj_chunk<NY, true>(th, o, u, ncells, stride, g, use_geom, t_guess, t_out, iters, stats,
+                           mv, guess_out, err, c * kUmmaM + threadIdx.x % kUmmaM, dsm, us, wg);
+  mlp_umma_teardown<kSatWg>(dsm, us.pending, us.phase);
 }
 
 }  // namespace
@@ -631,21 +680,24 @@ int launch_dt_finalize(double *d_dt, unsigned long long *acc, double cfl,
 int launch_satadj(const canoe_thermo_t &th, const canoe_satadj_opts_t &o, double *u,
                   int64_t ncells, int64_t stride, const Geom *g, const double *t_guess,
                   double *t_out, int32_t *iters, unsigned long long *stats,
-                  cudaStream_t st, const MlpView *mlp, double *guess_out) {
+                  cudaStream_t st, const MlpView *mlp, double *guess_out, uint32_t *err) {
   if (ncells <= 0) return 0;
   Geom gg{};
   if (g) gg = *g;
   MlpView mv{};
   if (mlp) mv = *mlp;
-  const unsigned nb = (unsigned)((ncells + 255) / 256);
   const int ug = g ? 1 : 0;
-#define CB_SAT(NY)                                                                        \
-  if (mlp)                                                                                \
-    k_satadj<NY, true><<<nb, 256, 0, st>>>(th, o, u, ncells, stride, gg, ug, t_guess, t_out, \
-                                           iters, stats, mv, guess_out);                  \
-  else                                                                                    \
-    k_satadj<NY, false><<<nb, 256, 0, st>>>(th, o, u, ncells, stride, gg, ug, t_guess, t_out, \
-                                            iters, stats, mv, guess_out)
+  int grid = 0;
+#define CB_SAT(NY)                                                                         \
+  if (mlp) {                                                                               \
+    CB_CUDA(umma_persistent_grid<kSatWg>(k_satadj_learned<NY>, (ncells + kUmmaM - 1) / kUmmaM, \
+                                         &grid));                                          \
+    k_satadj_learned<NY><<<grid, kSatWg * kUmmaM, UmmaLayout<kSatWg>::kBytes, st>>>(       \
+        th, o, u, ncells, stride, gg, ug, t_guess, t_out, iters, stats, mv, guess_out, err); \
+  } else {                                                                                 \
+    k_satadj<NY><<<(unsigned)((ncells + 255) / 256), 256, 0, st>>>(                        \
+        th, o, u, ncells, stride, gg, ug, t_guess, t_out, iters, stats);                   \
+  }
   switch (th.ny) {
     case 1: CB_SAT(1); break;
     case 2: CB_SAT(2); break;

@@ -6,9 +6,10 @@
 // weight gradients through shared memory (the 64 x 64 layer as a 128-deep
 // outer-product sum) and adds them to the global gradient with atomics.
 // Adam updates the FP32 master weights; a BF16 copy of w2 feeds the tensor
-// cores at inference.
+// cores (tcgen05, mlp.cuh) at inference.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -169,26 +170,48 @@ __global__ void k_mlp_forward(const float *__restrict__ p, const float *__restri
   y[s] = out;
 }
 
-// BF16 tensor-core inference (the warm-start path) on normalised inputs
-__global__ void __launch_bounds__(256)
+// BF16 tensor-core inference (the warm-start path's tcgen05 routines,
+// mlp.cuh) on normalised inputs: one persistent CTA of kInferWg warpgroups
+// per SM; the CTA stages the network and allocates its TMEM once, and
+// warpgroup g of CTA b takes the 128-sample chunks b kInferWg + g,
+// b kInferWg + g + gridDim.x kInferWg, ...  err receives CANOE_EBIT_TIMEOUT
+// if a warpgroup's bounded wait for its MMAs gave up; that warpgroup's
+// remaining outputs are NaN.
+constexpr int kInferWg = 8;  // 1024 threads, all 512 TMEM columns
+
+__global__ void __launch_bounds__(kInferWg * kUmmaM, 1)
     k_mlp_infer_tc(const float *__restrict__ p, const __nv_bfloat16 *__restrict__ w2h,
-                   const float *__restrict__ x, float *__restrict__ y, int64_t n) {
-  __shared__ float sw1[kMlpH * kMlpIn], sb1[kMlpH], sb2[kMlpH], sw3[kMlpH];
-  __shared__ __align__(16) __nv_bfloat16 sw2[kMlpH * kMlpH];
-  for (int q = threadIdx.x; q < kMlpH * kMlpIn; q += blockDim.x) sw1[q] = p[kMlpOffW1 + q];
-  for (int q = threadIdx.x; q < kMlpH; q += blockDim.x) {
-    sb1[q] = p[kMlpOffB1 + q];
-    sb2[q] = p[kMlpOffB2 + q];
-    sw3[q] = p[kMlpOffW3 + q];
-  }
-  for (int q = threadIdx.x; q < kMlpH * kMlpH; q += blockDim.x) sw2[q] = w2h[q];
-  __syncthreads();
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  float xs[kMlpIn];
+                   const float *__restrict__ x, float *__restrict__ y, int64_t n,
+                   uint32_t *err) {
+  extern __shared__ __align__(1024) uint8_t dsm[];
+  mlp_umma_setup<kInferWg>(dsm, p, w2h);
+  uint32_t phase = 0u;
+  bool live = true, pending = false;
+  const int wg = threadIdx.x / kUmmaM;
+  const int64_t nchunk = (n + kUmmaM - 1) / kUmmaM;
+  for (int64_t c = (int64_t)blockIdx.x * kInferWg + wg; c < nchunk;
+       c += (int64_t)gridDim.x * kInferWg) {
+    const int64_t s = c * kUmmaM + threadIdx.x % kUmmaM;
+    float xs[kMlpIn];
 #pragma unroll
-  for (int i = 0; i < kMlpIn; ++i) xs[i] = s < n ? x[s * kMlpIn + i] : 0.f;
-  const float out = mlp_warp_infer(xs, sw1, sb1, sw2, sb2, sw3, p[kMlpOffB3]);
-  if (s < n) y[s] = out;
+    for (int i = 0; i < kMlpIn; ++i) xs[i] = s < n ? x[s * kMlpIn + i] : 0.f;
+    const bool warp_run = __any_sync(0xffffffffu, s < n);
+    float out = __int_as_float(0x7fc00000);
+    if (live) {
+      bool ok = false;
+      const float o = mlp_umma_infer<kInferWg>(dsm, p, xs, warp_run, phase, &ok);
+      if (ok) {
+        phase ^= 1u;
+        out = o;
+      } else {
+        live = false;
+        pending = true;
+        if (threadIdx.x % kUmmaM == 0 && err) atomicOr(err, (uint32_t)CANOE_EBIT_TIMEOUT);
+      }
+    }
+    if (s < n) y[s] = out;
+  }
+  mlp_umma_teardown<kInferWg>(dsm, pending, phase);
 }
 
 }  // namespace
@@ -363,11 +386,14 @@ int canoe_mlp_forward(canoe_mlp_t m, const float *d_x, float *d_y, int64_t n, in
   if (!m || !d_x || !d_y || n < 0) return CANOE_ERR_ARG;
   if (n == 0) return 0;
   cudaStream_t st = (cudaStream_t)stream;
-  const unsigned nb = (unsigned)((n + 255) / 256);
-  if (tensor_core)
-    k_mlp_infer_tc<<<nb, 256, 0, st>>>(m->d_p, m->d_w2h, d_x, d_y, n);
-  else
-    k_mlp_forward<<<nb, 256, 0, st>>>(m->d_p, d_x, d_y, n);
+  if (tensor_core) {
+    // persistent: one CTA per SM
+    int grid = 0;
+    CB_CUDA(umma_persistent_grid<kInferWg>(k_mlp_infer_tc, (n + kUmmaM - 1) / kUmmaM, &grid));
+    k_mlp_infer_tc<<<grid, kInferWg * kUmmaM, UmmaLayout<kInferWg>::kBytes, st>>>(
+        m->d_p, m->d_w2h, d_x, d_y, n, nullptr);
+  } else
+    k_mlp_forward<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(m->d_p, d_x, d_y, n);
   CB_CUDA(cudaGetLastError());
   return 0;
 }

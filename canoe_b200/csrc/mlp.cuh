@@ -9,7 +9,11 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
+
+#include "bulk.cuh"
 
 namespace cb {
 
@@ -46,108 +50,322 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<uint32_t *>(&v);
 }
 
-// D = A * B + D, m16n8k16, A/B bf16, D fp32
-__device__ __forceinline__ void mma_bf16(float *d, const uint32_t *a, const uint32_t *b) {
+// ---------------------------------------------------------------------------
+// Inference on the 5th-generation tensor cores (tcgen05).
+//
+// One warpgroup (128 threads) infers 128 cells at a time as one M = 128 row
+// tile, one row (cell) per thread:
+//   layer 1 (4 -> 64, 2 % of the flops) runs in FP32 on the CUDA cores, each
+//     thread writing its row's 64 BF16 hidden values into the warpgroup's A
+//     tile in shared memory;
+//   layer 2 (64 -> 64) is four tcgen05.mma of K = 16, BF16 x BF16 with FP32
+//     accumulation into the warpgroup's 64 tensor-memory (TMEM) columns,
+//     row m in lane m;
+//   the epilogue reads each thread's row back with tcgen05.ld (warp w of a
+//     warpgroup reads TMEM lanes 32 w .. 32 w + 31), adds the bias, applies
+//     tanh and forms layer 3's dot product in registers.
+// The warpgroup's first thread issues its MMAs and commits them to the
+// warpgroup's mbarrier, which its threads wait on (bounded); the warpgroup
+// synchronises through its own named barrier (id 1 + warpgroup).
+//
+// The kernels that use it are persistent, one CTA of WG warpgroups per SM,
+// the warpgroups working on their own chunks without waiting on one
+// another.  On B200 a kernel holding TMEM instructions is resident at one
+// CTA per SM, whatever its registers and shared memory allow (the occupancy
+// query returns 1 for such a kernel and 3-5 for the same kernel without
+// them), so several small CTAs per SM are not available: an 8.4 M-cell
+// streaming kernel ran 0.076 ms plain, 0.31 ms with 256-thread CTAs that
+// merely contain an untaken tcgen05.alloc path, 0.59 ms with 128-thread
+// CTAs.  The CTA stages the weights and allocates its TMEM once
+// (mlp_umma_setup), each warpgroup infers any number of chunks
+// (mlp_umma_infer), and the CTA frees the columns at the end
+// (mlp_umma_teardown).
+//
+// Operands use the no-swizzle K-major canonical layout: 8-row x 16-byte core
+// matrices of 128 contiguous bytes; the 16-byte chunk holding elements
+// k = 8 kc .. 8 kc + 7 of row r of a `rows`-row operand sits at
+// kc * rows * 16 + (r / 8) * 128 + (r % 8) * 16.  In a shared-memory matrix
+// descriptor the stride between 8-row groups (SBO) is then 128 bytes and the
+// stride between the two K chunks of one MMA (LBO) rows * 16 bytes.
+
+constexpr int kUmmaM = 128;                      // rows per tile = threads per warpgroup
+constexpr int kUmmaABytes = kUmmaM * kMlpH * 2;  // one BF16 A tile, 16 KB
+constexpr int kUmmaBBytes = kMlpH * kMlpH * 2;   // BF16 w2, 8 KB
+
+// dynamic shared memory of a CTA of WG warpgroups: WG A tiles, w2, the FP32
+// weights, WG mbarriers and the TMEM address
+template <int WG>
+struct UmmaLayout {
+  static_assert(WG >= 1 && WG * kMlpH <= 512, "TMEM holds 512 columns");
+  static constexpr int kThreads = WG * kUmmaM;
+  static constexpr uint32_t kCols = WG * kMlpH <= 64    ? 64u
+                                    : WG * kMlpH <= 128 ? 128u
+                                    : WG * kMlpH <= 256 ? 256u
+                                                        : 512u;  // a power of two
+  static constexpr int kOffB = WG * kUmmaABytes;
+  static constexpr int kOffW = kOffB + kUmmaBBytes;  // w1, b1, b2, w3 (FP32)
+  static constexpr int kOffW1 = kOffW;
+  static constexpr int kOffB1 = kOffW1 + kMlpH * kMlpIn * 4;
+  static constexpr int kOffB2 = kOffB1 + kMlpH * 4;
+  static constexpr int kOffW3 = kOffB2 + kMlpH * 4;
+  static constexpr int kOffBar = kOffW3 + kMlpH * 4;
+  static constexpr int kOffTmem = kOffBar + WG * 8;
+  static constexpr int kBytes = kOffTmem + 16;
+};
+
+// instruction descriptor of tcgen05.mma kind::f16: FP32 D (bits 4-5 = 1),
+// BF16 A (bits 7-9 = 1) and B (bits 10-12 = 1), both K-major (bits 15, 16 =
+// 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28
+constexpr uint32_t kUmmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                                ((uint32_t)(kMlpH >> 3) << 17) | ((uint32_t)(kUmmaM >> 4) << 24);
+
+// named-barrier reductions over `n` threads (a warpgroup): every thread
+// gets the OR / AND of v
+__device__ __forceinline__ bool bar_red_or(int id, int n, bool v) {
+  uint32_t r;
   asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, %2, %3, q;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
 }
 
-// Warp-cooperative inference for the warp's 32 samples (one per lane).
-// x: this lane's normalised input (kMlpIn).  Shared memory sw1/sb1/sb2/sw3
-// hold the FP32 parameters, sw2 the BF16 w2.  Returns this lane's
-// normalised output.  Layer 1 runs in FP32 on the CUDA cores directly into
-// the A-operand layout of layer 2; layer 2 (the 64 x 64 product, 97 % of the
-// flops) runs on the tensor cores; its accumulators feed layer 3's dot
-// product.
-__device__ __forceinline__ float mlp_warp_infer(const float *x, const float *sw1,
-                                                const float *sb1,
-                                                const __nv_bfloat16 *sw2,
-                                                const float *sb2, const float *sw3,
-                                                float b3) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  // inputs of rows g, g+8, g+16, g+24
-  float xr[4][kMlpIn];
+__device__ __forceinline__ bool bar_red_and(int id, int n, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.and.pred p, %2, %3, q;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ uint32_t umma_chunk(int r, int kc, int rows) {
+  return (uint32_t)kc * (uint32_t)(rows * 16) + (uint32_t)(r >> 3) * 128u + (uint32_t)(r & 7) * 16u;
+}
+
+// shared-memory matrix descriptor: start address, LBO and SBO in 16-byte
+// units (bits 0-13, 16-29, 32-45), descriptor version 1 (bits 46-47), base
+// offset 0, no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_addr(dst)),
+               "r"(ncols)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// D(tmem) = A * B^T (+ D when accumulate), A and B from shared memory
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// arrive on mbarrier m once every MMA this thread issued has completed
+__device__ __forceinline__ void umma_commit(uint64_t *m) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_addr(m))
+               : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane, then the wait
+// that completes the load (the registers are tied to the wait so no use of
+// them can be scheduled before it)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile(
+      "tcgen05.wait::ld.sync.aligned;"
+      : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+        "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]),
+        "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+      :
+      : "memory");
+}
+
+// Once per CTA, by every thread (CTA-uniform): stage the weights, allocate
+// the CTA's TMEM columns, initialise the warpgroups' mbarriers.
+template <int WG>
+__device__ __forceinline__ void mlp_umma_setup(uint8_t *sm, const float *p,
+                                               const __nv_bfloat16 *w2h) {
+  using L = UmmaLayout<WG>;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  float *w1 = reinterpret_cast<float *>(sm + L::kOffW1);
+  float *b1 = reinterpret_cast<float *>(sm + L::kOffB1);
+  float *b2 = reinterpret_cast<float *>(sm + L::kOffB2);
+  float *w3 = reinterpret_cast<float *>(sm + L::kOffW3);
+  for (int q = tid; q < kMlpH * kMlpIn; q += L::kThreads) w1[q] = p[kMlpOffW1 + q];
+  for (int q = tid; q < kMlpH; q += L::kThreads) {
+    b1[q] = p[kMlpOffB1 + q];
+    b2[q] = p[kMlpOffB2 + q];
+    w3[q] = p[kMlpOffW3 + q];
+  }
+  // w2 is row-major [out n][in k]: rows of B with K contiguous (K-major)
+  for (int q = tid; q < kMlpH * kMlpH / 8; q += L::kThreads) {
+    const int n = q >> 3, kc = q & 7;
+    *reinterpret_cast<uint4 *>(sm + L::kOffB + umma_chunk(n, kc, kMlpH)) =
+        *reinterpret_cast<const uint4 *>(w2h + n * kMlpH + kc * 8);
+  }
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L::kOffBar);
+  if (warp == 0) {
+    tmem_alloc(reinterpret_cast<uint32_t *>(sm + L::kOffTmem), L::kCols);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    for (int g = 0; g < WG; ++g) mbar_init(&bar[g], 1);
+    fence_mbar_init();
+  }
+  fence_proxy_async();  // B's generic-proxy writes, before the tensor cores read them
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+}
+
+// Inference of one chunk of 128 cells by the calling warpgroup (all 128 of
+// its threads together; the other warpgroups are not involved).
+//   x        this thread's normalised input (zeros where the cell is absent)
+//   warp_run warp-uniform: whether a lane of this warp wants its result; a
+//            warp that does not skips its rows' layer 1 and the TMEM read
+//   phase    the phase of the warpgroup's mbarrier for this chunk: 0 for the
+//            warpgroup's first inference, flipped after each one
+// Returns the thread's normalised output and sets *ok (the same on every
+// thread of the warpgroup); on false, the bounded wait for the MMAs gave up,
+// the result is absent, and the warpgroup must not call this again
+// (mlp_umma_teardown waits for the MMAs once more before TMEM is freed).
+template <int WG>
+__device__ __forceinline__ float mlp_umma_infer(uint8_t *sm, const float *p, const float *x,
+                                                bool warp_run, uint32_t phase, bool *ok) {
+  using L = UmmaLayout<WG>;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int wg = tid / kUmmaM, row = tid % kUmmaM;
+  const float *w1 = reinterpret_cast<const float *>(sm + L::kOffW1);
+  const float *b1 = reinterpret_cast<const float *>(sm + L::kOffB1);
+  const float *b2 = reinterpret_cast<const float *>(sm + L::kOffB2);
+  const float *w3 = reinterpret_cast<const float *>(sm + L::kOffW3);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L::kOffBar) + wg;
+  uint8_t *at = sm + wg * kUmmaABytes;
+  // layer 1 of this thread's row, FP32, into the A tile as BF16
+  if (warp_run) {
+#pragma unroll 2
+    for (int kc = 0; kc < kMlpH / 8; ++kc) {
+      float h[8];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+      for (int j = 0; j < 8; ++j) {
+        const int c = 8 * kc + j;
+        float a = b1[c];
 #pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) xr[r][i] = __shfl_sync(0xffffffffu, x[i], g + 8 * r);
-  // layer 1 into A fragments: afr[mt][kt][4] (mt = m-tile of 16 rows)
-  uint32_t afr[2][4][4];
-#pragma unroll
-  for (int kt = 0; kt < 4; ++kt) {
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {  // cols 16kt + 2t + {0,1} (+8)
-      const int c0 = 16 * kt + 2 * t + 8 * half;
-      float h[4][2];
-#pragma unroll
-      for (int cc = 0; cc < 2; ++cc) {
-        const int c = c0 + cc;
-        const float bb = sb1[c];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          float a = bb;
-#pragma unroll
-          for (int i = 0; i < kMlpIn; ++i) a = fmaf(sw1[c * kMlpIn + i], xr[r][i], a);
-          h[r][cc] = tanh_fast(a);
-        }
+        for (int i = 0; i < kMlpIn; ++i) a = fmaf(w1[c * kMlpIn + i], x[i], a);
+        h[j] = tanh_fast(a);
       }
-      // A regs: a0 (row g, cols lo), a1 (row g+8, cols lo), a2 (row g, cols hi),
-      // a3 (row g+8, cols hi)
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-        afr[mt][kt][half * 2 + 0] = pack_bf16(h[2 * mt][0], h[2 * mt][1]);
-        afr[mt][kt][half * 2 + 1] = pack_bf16(h[2 * mt + 1][0], h[2 * mt + 1][1]);
-      }
+      uint4 v;
+      v.x = pack_bf16(h[0], h[1]);
+      v.y = pack_bf16(h[2], h[3]);
+      v.z = pack_bf16(h[4], h[5]);
+      v.w = pack_bf16(h[6], h[7]);
+      *reinterpret_cast<uint4 *>(at + umma_chunk(row, kc, kUmmaM)) = v;
     }
   }
-  // layer 2: acc[mt][nt][4]
-  float y[4] = {0.f, 0.f, 0.f, 0.f};  // partial layer-3 sums of rows g+8r
+  // A's generic-proxy writes before the tensor cores read them; the previous
+  // chunk's TMEM reads before this chunk's MMAs overwrite the accumulators
+  fence_proxy_async();
+  tc_fence_before();
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(kUmmaM) : "memory");
+  const uint32_t tm = *reinterpret_cast<const uint32_t *>(sm + L::kOffTmem);
+  const uint32_t dcol = tm + (uint32_t)(wg * kMlpH);
+  if (row == 0) {
+    tc_fence_after();
+    const uint32_t a0 = smem_addr(at), b0 = smem_addr(sm + L::kOffB);
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
-    float acc[2][4];
-    const int n0 = 8 * nt + 2 * t;
+    for (int ks = 0; ks < kMlpH / 16; ++ks)
+      umma_bf16(dcol, umma_desc(a0 + ks * 2 * (kUmmaM * 16), kUmmaM * 16, 128),
+                umma_desc(b0 + ks * 2 * (kMlpH * 16), kMlpH * 16, 128), kUmmaIdesc,
+                ks > 0 ? 1u : 0u);
+    umma_commit(bar);
+  }
+  const bool done = bar_red_and(1 + wg, kUmmaM, mbar_wait(bar, phase));
+  tc_fence_after();
+  float y = 0.f;
+  if (done && warp_run) {
+    const uint32_t ta = dcol + ((uint32_t)(32 * (warp & 3)) << 16);
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-      acc[mt][0] = sb2[n0];
-      acc[mt][1] = sb2[n0 + 1];
-      acc[mt][2] = sb2[n0];
-      acc[mt][3] = sb2[n0 + 1];
-    }
+    for (int c0 = 0; c0 < kMlpH; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(ta + (uint32_t)c0, r);
 #pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      // B fragment: B[k][n] = w2[n][k], n = 8 nt + g, k = 16 kt + 2t (+1), +8
-      const __nv_bfloat16 *wr = sw2 + (8 * nt + g) * kMlpH + 16 * kt + 2 * t;
-      uint32_t bfr[2];
-      bfr[0] = *reinterpret_cast<const uint32_t *>(wr);
-      bfr[1] = *reinterpret_cast<const uint32_t *>(wr + 8);
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) mma_bf16(acc[mt], afr[mt][kt], bfr);
-    }
-    const float w3a = sw3[n0], w3b = sw3[n0 + 1];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-      y[2 * mt] += w3a * tanh_fast(acc[mt][0]) + w3b * tanh_fast(acc[mt][1]);
-      y[2 * mt + 1] += w3a * tanh_fast(acc[mt][2]) + w3b * tanh_fast(acc[mt][3]);
+      for (int j = 0; j < 16; ++j)
+        y = fmaf(w3[c0 + j], tanh_fast(__uint_as_float(r[j]) + b2[c0 + j]), y);
     }
   }
-  // reduce over the quad (t = 0..3)
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    y[r] += __shfl_xor_sync(0xffffffffu, y[r], 1);
-    y[r] += __shfl_xor_sync(0xffffffffu, y[r], 2);
+  *ok = done;
+  return y + p[kMlpOffB3];
+}
+
+// Once per CTA at the end, by every thread (CTA-uniform).  pending: the
+// warpgroup's last MMAs were not seen to complete (phase: that chunk's
+// phase); they get one more bounded wait before the columns are freed.
+template <int WG>
+__device__ __forceinline__ void mlp_umma_teardown(uint8_t *sm, bool pending, uint32_t phase) {
+  using L = UmmaLayout<WG>;
+  if (pending && threadIdx.x % kUmmaM == 0)
+    mbar_wait(reinterpret_cast<uint64_t *>(sm + L::kOffBar) + threadIdx.x / kUmmaM, phase);
+  tc_fence_before();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) {
+    tc_fence_after();
+    tmem_dealloc(*reinterpret_cast<const uint32_t *>(sm + L::kOffTmem), L::kCols);
   }
-  // lane l holds row l: quad of g' = l % 8, slot r = l / 8
-  float out = 0.f;
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const float v = __shfl_sync(0xffffffffu, y[r], 4 * (lane & 7));
-    if ((lane >> 3) == r) out = v;
-  }
-  return out + b3;
+}
+
+// Grid of a persistent tcgen05 kernel of WG warpgroups per CTA: one CTA per
+// SM (the residency of a kernel holding TMEM instructions), no more CTAs
+// than chunks of 128 cells need; also raises the kernel's dynamic shared
+// memory limit to the layout's size.
+template <int WG, class K>
+inline cudaError_t umma_persistent_grid(K kernel, int64_t nchunk, int *grid) {
+  int dev = 0, sms = 0;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) ||
+      (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) ||
+      (e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                UmmaLayout<WG>::kBytes)))
+    return e;
+  *grid = (int)std::max<int64_t>(1, std::min<int64_t>((nchunk + WG - 1) / WG, sms));
+  return cudaSuccess;
 }
 
 }  // namespace cb

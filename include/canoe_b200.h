@@ -226,7 +226,9 @@ int canoe_mlp_loss_grad(canoe_mlp_t m, const float *d_x, const float *d_y, int64
 int canoe_mlp_adam_step(canoe_mlp_t m, float lr, float beta1, float beta2, float eps,
                         void *stream);
 /* normalised forward pass: FP32 CUDA cores (tensor_core = 0) or the BF16
- * tensor-core path of the warm start (tensor_core = 1) */
+ * tensor-core path of the warm start (tensor_core = 1: tcgen05 MMAs with the
+ * layer-2 accumulator in tensor memory; an output is NaN if its CTA's bounded
+ * wait for the MMAs gave up) */
 int canoe_mlp_forward(canoe_mlp_t m, const float *d_x, float *d_y, int64_t n, int tensor_core,
                       void *stream);
 /* canoe_saturation_adjust with the network's guess as the starting point
