@@ -490,7 +490,7 @@ struct UmmaState {
 // registers across the Newton iteration of every warp.
 constexpr int kSatWg = 6;  // warpgroups per CTA of the learned adjustment (24 warps)
 
-__device__ __noinline__ float mlp_infer_call(uint8_t *sm, const float *p, const float *x,
+__device__ __forceinline__ float mlp_infer_call(uint8_t *sm, const float *p, const float *x,
                                              bool warp_run, uint32_t phase, bool *ok) {
   return mlp_umma_infer<kSatWg>(sm, p, x, warp_run, phase, ok);
 }
