@@ -536,6 +536,8 @@ def c5_report(net, steps=5, warmup=2):
                      "sequential_value": cells / (ms_seq * 1e-3),
                      "threads_per_pencil": {str(t): int((choice == t).sum())
                                             for t in (64, 96, 128, 160, 192, 256)},
+                     "cells_per_flux_run": {str(r): sum(1 for _, fr in bt.shapes() if fr == r)
+                                            for r in (0, 8, 16, 32, 64)},
                      "error_words": int(np.bitwise_or.reduce(np.array(errs)))}
         bt.close()
         for b in blocks:

@@ -108,6 +108,8 @@ SIGNATURES = [
                                     ctypes.c_float, c_void_p]),
     ("canoe_mlp_forward", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
     ("canoe_block_set_column_threads", c_int, [c_void_p, c_int]),
+    ("canoe_block_set_flux_run", c_int, [c_void_p, c_int]),
+    ("canoe_block_get_shapes", c_int, [c_void_p, c_void_p, c_void_p]),
     ("canoe_selftest_bounded_wait", c_int, [c_int, c_int, c_void_p]),
     ("canoe_measure_fma_peak", c_int, [c_int, POINTER(c_double)]),
     ("canoe_block_set_neighbor", c_int, [c_void_p, c_int, c_void_p]),

@@ -48,3 +48,15 @@ class Batch:
         out = np.zeros(len(self.blocks), dtype=np.int32)
         check(self.lib.canoe_batch_autotune(self.h, out.ctypes.data), "canoe_batch_autotune")
         return out
+
+    def shapes(self):
+        """(threads per x1 pencil, cells per x2 / x3 flux run) of every block
+        (0 = the default)."""
+        import ctypes
+        out = []
+        for b in self.blocks:
+            t, r = ctypes.c_int32(0), ctypes.c_int32(0)
+            check(self.lib.canoe_block_get_shapes(b.h, ctypes.byref(t), ctypes.byref(r)),
+                  "canoe_block_get_shapes")
+            out.append((t.value, r.value))
+        return out

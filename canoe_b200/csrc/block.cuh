@@ -37,6 +37,10 @@ struct Geom {
   // threads per x1 pencil (a multiple of 32 in 64..160; 0 = 160), chosen
   // per block by canoe_batch_autotune
   int col_threads;
+  // cells per thread of the x2 / x3 register-window flux runs (4..256; 0 =
+  // 16 in FP32, 32 in FP64), chosen per block by canoe_batch_autotune; the
+  // results do not depend on it
+  int flux_run = 0;
   // x1 pencil launches over npanel equal blocks stored pstride doubles apart
   // (the six panels of a cubed-sphere shell share one geometry)
   int npanel = 1;

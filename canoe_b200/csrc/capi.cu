@@ -762,6 +762,27 @@ int canoe_block_set_column_threads(canoe_block_t b, int threads) {
   return 0;
 }
 
+int canoe_block_set_flux_run(canoe_block_t b, int cells) {
+  if (!b) return CANOE_ERR_ARG;
+  if (cells != 0 && (cells < 4 || cells > 256)) {
+    set_error("cells per x2 / x3 flux run must be in 4..256 (0: default)");
+    return CANOE_ERR_ARG;
+  }
+  b->g.flux_run = cells;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return 0;
+}
+
+int canoe_block_get_shapes(canoe_block_t b, int32_t *col_threads, int32_t *flux_run) {
+  if (!b) return CANOE_ERR_ARG;
+  if (col_threads) *col_threads = b->g.col_threads;
+  if (flux_run) *flux_run = b->g.flux_run;
+  return 0;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -1208,45 +1229,62 @@ int canoe_batch_synchronize(canoe_batch_t q) {
   return 0;
 }
 
-// Per block, time steps with each candidate number of threads per x1
-// pencil (64 .. 256) and keep the fastest; the blocks' states, dt
-// and counters are restored afterwards.  h_threads (may be NULL) receives
-// the choices.
+// Per block, time steps of the block alone with each candidate number of
+// threads per x1 pencil (64 .. 256) and keep the fastest; then time steps of
+// the whole batch with each candidate number of cells per x2 / x3 flux run
+// (the default, 8 .. 64) and keep the fastest for every block.  The blocks'
+// states, dt and counters are restored afterwards.  h_threads (may be NULL)
+// receives the thread choices; canoe_block_get_shapes gives both.
 int canoe_batch_autotune(canoe_batch_t q, int32_t *h_threads) {
   if (!q) return CANOE_ERR_ARG;
   static const int cand[] = {64, 96, 128, 160, 192, 256};
+  static const int run_cand[] = {0, 8, 16, 32, 64};
+  const size_t nb = q->blocks.size();
   cudaEvent_t e0, e1;
   CB_CUDA(cudaEventCreate(&e0));
   CB_CUDA(cudaEventCreate(&e1));
+  // every block's state, kept until the batch-wide sweep is done
+  std::vector<double *> su(nb, nullptr), sw(nb, nullptr);
+  std::vector<double> dts(2 * nb, 0.);
   int rc = 0;
-  for (size_t n = 0; n < q->blocks.size() && !rc; ++n) {
+  for (size_t n = 0; n < nb && !rc; ++n) {
     canoe_block *b = q->blocks[n];
     const size_t bytes = b->nvals * sizeof(double);
-    double *su = nullptr, *sw = nullptr, dts[2];
-    if (cudaMalloc(&su, bytes) || cudaMalloc(&sw, bytes)) {
+    if (cudaMalloc(&su[n], bytes) || cudaMalloc(&sw[n], bytes)) {
       rc = cuda_status(cudaErrorMemoryAllocation, "canoe_batch_autotune");
       break;
     }
-    cudaMemcpyAsync(su, b->d_u, bytes, cudaMemcpyDeviceToDevice, b->st);
-    cudaMemcpyAsync(sw, b->d_w, bytes, cudaMemcpyDeviceToDevice, b->st);
-    cudaMemcpyAsync(dts, b->d_dt, sizeof(dts), cudaMemcpyDeviceToHost, b->st);
+    cudaMemcpyAsync(su[n], b->d_u, bytes, cudaMemcpyDeviceToDevice, b->st);
+    cudaMemcpyAsync(sw[n], b->d_w, bytes, cudaMemcpyDeviceToDevice, b->st);
+    cudaMemcpyAsync(&dts[2 * n], b->d_dt, 2 * sizeof(double), cudaMemcpyDeviceToHost, b->st);
     cudaStreamSynchronize(b->st);
-    float best = 1e30f;
+  }
+  auto restore = [&](size_t n) {
+    canoe_block *b = q->blocks[n];
+    const size_t bytes = b->nvals * sizeof(double);
+    cudaMemcpyAsync(b->d_u, su[n], bytes, cudaMemcpyDeviceToDevice, b->st);
+    cudaMemcpyAsync(b->d_w, sw[n], bytes, cudaMemcpyDeviceToDevice, b->st);
+    cudaMemcpyAsync(b->d_dt, &dts[2 * n], 2 * sizeof(double), cudaMemcpyHostToDevice, b->st);
+    cudaStreamSynchronize(b->st);
+  };
+  // threads per x1 pencil, block by block: one warm-up step, then two timed
+  // steps of the block alone, with the default flux runs
+  for (size_t n = 0; n < nb && !rc; ++n) {
+    canoe_block *b = q->blocks[n];
+    float best = 1e30f, ms = 0.f;
     int pick = kColThreads;
+    b->g.flux_run = 0;
     for (int c : cand) {
       b->g.col_threads = c;
-      if ((rc = step_launches(b, 0.))) break;
-      cudaEventRecord(e0, b->st);
-      for (int r = 0; r < 2 && !rc; ++r) rc = step_launches(b, 0.);
-      cudaEventRecord(e1, b->st);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      // restore the state for the next candidate
-      cudaMemcpyAsync(b->d_u, su, bytes, cudaMemcpyDeviceToDevice, b->st);
-      cudaMemcpyAsync(b->d_w, sw, bytes, cudaMemcpyDeviceToDevice, b->st);
-      cudaMemcpyAsync(b->d_dt, dts, sizeof(dts), cudaMemcpyHostToDevice, b->st);
-      cudaStreamSynchronize(b->st);
+      rc = step_launches(b, 0.);
+      if (!rc) {
+        cudaEventRecord(e0, b->st);
+        for (int k = 0; k < 2 && !rc; ++k) rc = step_launches(b, 0.);
+        cudaEventRecord(e1, b->st);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+      }
+      restore(n);
       if (rc) break;
       if (ms < best) {
         best = ms;
@@ -1254,6 +1292,36 @@ int canoe_batch_autotune(canoe_batch_t q, int32_t *h_threads) {
       }
     }
     b->g.col_threads = pick;
+    if (h_threads) h_threads[n] = pick;
+  }
+  // cells per x2 / x3 flux run, for the batch as a whole: the blocks share
+  // the GPU when the batch steps, so a block timed alone favours shorter
+  // runs (more CTAs) than pay off in the batch
+  if (!rc) {
+    float best = 1e30f, ms = 0.f;
+    int run_pick = 0;
+    for (int c : run_cand) {
+      for (canoe_block *b : q->blocks) b->g.flux_run = c;
+      rc = batch_launches(q);
+      if (!rc) {
+        cudaEventRecord(e0, q->st);
+        for (int k = 0; k < 2 && !rc; ++k) rc = batch_launches(q);
+        cudaEventRecord(e1, q->st);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+      }
+      cudaStreamSynchronize(q->st);
+      for (size_t n = 0; n < nb; ++n) restore(n);
+      if (rc) break;
+      if (ms < best) {
+        best = ms;
+        run_pick = c;
+      }
+    }
+    for (canoe_block *b : q->blocks) b->g.flux_run = run_pick;
+  }
+  for (size_t n = 0; n < nb; ++n) {
+    canoe_block *b = q->blocks[n];
     if (b->gexec) {
       cudaGraphExecDestroy(b->gexec);
       b->gexec = nullptr;
@@ -1261,9 +1329,8 @@ int canoe_batch_autotune(canoe_batch_t q, int32_t *h_threads) {
     cudaMemsetAsync(b->d_sat, 0, 4 * sizeof(unsigned long long), b->st);
     cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), b->st);
     cudaStreamSynchronize(b->st);
-    cudaFree(su);
-    cudaFree(sw);
-    if (h_threads) h_threads[n] = pick;
+    if (su[n]) cudaFree(su[n]);
+    if (sw[n]) cudaFree(sw[n]);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -150,7 +150,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3)
 // are issued one step ahead.  Every slope, interface value, flux and
 // difference is the tile kernel's expression on the same operands, so both
 // give the same bits.
-// cells per run: 16 in FP32, 32 in FP64 (measured on C2 128x256x256: x2
+// default cells per run (Geom::flux_run overrides it): 16 in FP32, 32 in
+// FP64 (measured on C2 128x256x256: x2
 // 0.343 / 0.355 / 0.365 ms per FP32 launch at 16 / 32 / 8 cells, FP64 0.732
 // / 0.714 / 0.790 ms)
 template <typename R>
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(32 * RBY)
   if (i > g.ie || o > (DIR == 1 ? g.ke : g.je)) return;
   const int dlo = DIR == 1 ? g.js : g.ks;
   const int dhi = DIR == 1 ? g.je : g.ke;
-  constexpr int RL = run_len<R>();
+  const int RL = g.flux_run > 0 ? g.flux_run : run_len<R>();
   const int s0 = dlo + blockIdx.z * RL;
   const int s1 = min(s0 + RL, dhi + 1);  // one past the run's last cell
   const int64_t sd = DIR == 1 ? g.nc1 : g.sk;
@@ -307,7 +308,7 @@ int run_x23(const Geom &g, const canoe_thermo_t &th, const double *w, double *du
             const double *dtp, double beta, double *fo, cudaStream_t st) {
   const int nd = DIR == 1 ? g.nx2 : g.nx3;
   const int no = DIR == 1 ? g.nx3 : g.nx2;
-  constexpr int RL = run_len<R>();
+  const int RL = g.flux_run > 0 ? g.flux_run : run_len<R>();
   // a 2-D block (one line across the flux direction) keeps the tile kernel:
   // its runs would fill one warp in four of each CTA, and the 150 x 100
   // bubble would march 20 warps in all (x2 pass 4 x slower than the tiles);

@@ -376,6 +376,17 @@ int canoe_block_error_word(canoe_block_t b, uint32_t *bits);
  * counterpart (the reference sweeps columns serially). */
 int canoe_block_set_column_threads(canoe_block_t b, int threads);
 
+/* Cells per thread of the x2 / x3 register-window flux runs (4..256; 0 = 16
+ * with the FP32 flux path, 32 in FP64).  The results do not depend on it.
+ * No reference counterpart: the reference's CalculateFluxes loops over
+ * whole pencils (patches/19.calculate_fluxes.patch). */
+int canoe_block_set_flux_run(canoe_block_t b, int cells);
+
+/* The block's launch shapes: threads per x1 pencil and cells per x2 / x3
+ * flux run (0 = the defaults), as set or as canoe_batch_autotune chose them.
+ * No reference counterpart. */
+int canoe_block_get_shapes(canoe_block_t b, int32_t *col_threads, int32_t *flux_run);
+
 /* ---------------- batches of uneven blocks ----------------
  * Steps many blocks as one CUDA graph whose branches (one per block, on the
  * block's own stream) run concurrently; each block uses its own device dt
@@ -448,8 +459,11 @@ int canoe_batch_destroy(canoe_batch_t q);
 int canoe_batch_use_graph(canoe_batch_t q, int on);
 int canoe_batch_step(canoe_batch_t q);
 int canoe_batch_synchronize(canoe_batch_t q);
-/* pick the fastest threads per x1 pencil of every block by timing; the
- * blocks' states are restored; h_threads[n] (may be NULL) gets the choices */
+/* pick, by timing, the fastest threads per x1 pencil of every block (each
+ * block timed alone) and then the fastest cells per x2 / x3 flux run for the
+ * batch (the whole batch timed); the blocks' states are restored;
+ * h_threads[n] (may be NULL) gets the thread choices, canoe_block_get_shapes
+ * both */
 int canoe_batch_autotune(canoe_batch_t q, int32_t *h_threads);
 
 /* ---------------- cubed-sphere shell (exo3) ----------------

@@ -53,6 +53,7 @@ def test_autotune_keeps_state_and_results():
     bt = Batch(blocks)
     choice = bt.autotune()
     assert all(c in (64, 96, 128, 160, 192, 256) for c in choice)
+    assert all(t == c and r in (0, 8, 16, 32, 64) for (t, r), c in zip(bt.shapes(), choice))
     for b, u in zip(blocks, u0):
         assert np.array_equal(b.conserved(), u)
     bt.step()
@@ -83,3 +84,38 @@ def test_column_threads_do_not_change_results(flag):
         b.close()
     for o in out[1:]:
         assert np.array_equal(o, out[0])
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_flux_run_length_does_not_change_results(precision):
+    """Any number of cells per x2 / x3 flux run gives the same bits, in FP64
+    and on the FP32 flux path."""
+    from canoe_b200 import problems
+    from canoe_b200._abi import check, load
+    lib = load()
+    out = []
+    for cells in (0, 4, 8, 16, 64):
+        p = problems.moist3d(nx1=24, nx2=40, nx3=36, x1max=3000.0, x2max=4000.0,
+                             x3max=3600.0, noise=0.5)
+        p.cfg.precision = precision
+        b = MeshBlock(p)
+        check(lib.canoe_block_set_flux_run(b.h, cells))
+        b.step(1.0)
+        b.step(1.0)
+        out.append(b.conserved())
+        assert b.error_word() == 0
+        b.close()
+    for o in out[1:]:
+        assert np.array_equal(o, out[0])
+
+
+def test_flux_run_rejects_out_of_range():
+    from canoe_b200 import problems
+    from canoe_b200._abi import load
+    lib = load()
+    b = MeshBlock(problems.moist3d(nx1=16, nx2=8, nx3=8, x1max=2000.0, x2max=800.0,
+                                   x3max=800.0))
+    assert lib.canoe_block_set_flux_run(b.h, 3) != 0
+    assert lib.canoe_block_set_flux_run(b.h, 257) != 0
+    assert lib.canoe_block_set_flux_run(b.h, 0) == 0
+    b.close()
