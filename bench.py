@@ -362,6 +362,31 @@ def c4_report(net, th, ncells=1 << 24, reps=3):
         out[name] = {"ms": ms, "evaluations_per_cell": float(s[1]) / s[0],
                      "fallback_rate": float(s[2]) / s[0], "not_converged": int(s[3])}
         del d
+    # the network's inference alone over the same number of cells (seeded
+    # normalised inputs): tcgen05 warpgroups against the FP32 CUDA cores
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    x = torch.randn(ncells, 4, device="cuda", dtype=torch.float32, generator=gen)
+    y = torch.empty(ncells, device="cuda", dtype=torch.float32)
+    inf = {}
+    for name, tc in (("tcgen05", 1), ("fp32_cuda_cores", 0)):
+        def fwd():
+            check(lib.canoe_mlp_forward(net.h, x.data_ptr(), y.data_ptr(), ncells, tc, None))
+        for _ in range(3):
+            fwd()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fwd()
+        e1.record()
+        e1.synchronize()
+        inf[name + "_ms"] = e0.elapsed_time(e1) / reps
+        if tc:
+            inf["finite"] = bool(torch.isfinite(y).all())
+    inf["samples_per_s"] = ncells / (inf["tcgen05_ms"] * 1e-3)
+    out["inference"] = inf
+    del x, y
     out["note"] = ("same tolerance (1e-8 K + one polishing step) and the same answer; "
                    "the gated start uses the network where it predicts latent heating")
     return out
