@@ -111,6 +111,7 @@ SIGNATURES = [
     ("canoe_block_set_flux_run", c_int, [c_void_p, c_int]),
     ("canoe_block_get_shapes", c_int, [c_void_p, c_void_p, c_void_p]),
     ("canoe_selftest_bounded_wait", c_int, [c_int, c_int, c_void_p]),
+    ("canoe_selftest_umma_wait", c_int, [c_int, c_int, c_void_p]),
     ("canoe_measure_fma_peak", c_int, [c_int, POINTER(c_double)]),
     ("canoe_block_set_neighbor", c_int, [c_void_p, c_int, c_void_p]),
     ("canoe_block_stage", c_int, [c_void_p, c_int, c_double]),

@@ -4,6 +4,7 @@
 // Nothing faults: the barrier's phase is completed before the kernel exits.
 #include "block.cuh"
 #include "bulk.cuh"
+#include "mlp.cuh"
 
 namespace cb {
 namespace {
@@ -35,6 +36,89 @@ extern "C" int canoe_selftest_bounded_wait(int spins, int complete, uint32_t *h_
   cudaError_t e = cudaMemset(d, 0, sizeof(uint32_t));
   if (e == cudaSuccess) {
     k_bounded_wait<<<1, 32>>>(d, spins, complete ? 2 : 1);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(h_bits, d, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  CB_CUDA(e);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The same for the tensor-core completion wait of the warm-start inference
+// (mlp.cuh): one warpgroup allocates TMEM, issues the layer-2 MMAs on zero
+// operands and commits them to its mbarrier when `issue` is set, and waits a
+// bounded number of polls.  Without the MMAs nothing can complete the phase:
+// the wait must give up with CANOE_EBIT_TIMEOUT, and the columns are freed
+// safely because nothing is in flight.  With them the wait must succeed and
+// the accumulator must read back as zeros (CANOE_EBIT_NAN otherwise).
+
+namespace cb {
+namespace {
+
+__global__ void __launch_bounds__(kUmmaM, 1) k_umma_wait(uint32_t *err, int spins, int issue) {
+  __shared__ __align__(128) uint8_t a[kUmmaABytes];
+  __shared__ __align__(128) uint8_t b[kUmmaBBytes];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tm_slot;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (int q = tid; q < kUmmaABytes / 16; q += kUmmaM) reinterpret_cast<uint4 *>(a)[q] = zero;
+  for (int q = tid; q < kUmmaBBytes / 16; q += kUmmaM) reinterpret_cast<uint4 *>(b)[q] = zero;
+  if (warp == 0) {
+    tmem_alloc(&tm_slot, (uint32_t)kMlpH);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tm = tm_slot;
+  if (tid == 0 && issue) {
+    const uint32_t a0 = smem_addr(a), b0 = smem_addr(b);
+    for (int ks = 0; ks < kMlpH / 16; ++ks)
+      umma_bf16(tm, umma_desc(a0 + ks * 2 * (kUmmaM * 16), kUmmaM * 16, 128),
+                umma_desc(b0 + ks * 2 * (kMlpH * 16), kMlpH * 16, 128), kUmmaIdesc,
+                ks > 0 ? 1u : 0u);
+    umma_commit(&bar);
+  }
+  const bool done = __syncthreads_and(mbar_wait(&bar, 0, spins));
+  if (!done && tid == 0) atomicOr(err, (uint32_t)CANOE_EBIT_TIMEOUT);
+  tc_fence_after();
+  if (done) {
+    uint32_t r[16];
+    tmem_ld16(tm + ((uint32_t)(32 * warp) << 16), r);
+    bool nz = false;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) nz = nz || r[j] != 0u;
+    if (nz) atomicOr(err, (uint32_t)CANOE_EBIT_NAN);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tm, (uint32_t)kMlpH);
+  }
+}
+
+}  // namespace
+}  // namespace cb
+
+extern "C" int canoe_selftest_umma_wait(int spins, int issue, uint32_t *h_bits) {
+  using namespace cb;
+  if (!h_bits || spins < 1 || spins > (1 << 20)) {
+    set_error("canoe_selftest_umma_wait: spins in 1..2^20 and a result pointer");
+    return CANOE_ERR_ARG;
+  }
+  uint32_t *d = nullptr;
+  CB_CUDA(cudaMalloc(&d, sizeof(uint32_t)));
+  cudaError_t e = cudaMemset(d, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) {
+    k_umma_wait<<<1, kUmmaM>>>(d, spins, issue ? 1 : 0);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(h_bits, d, sizeof(uint32_t), cudaMemcpyDeviceToHost);

@@ -162,6 +162,15 @@ int canoe_device_sm_count(int *out);
  * counterpart (the reference has no device waits). */
 int canoe_selftest_bounded_wait(int spins, int complete, uint32_t *h_bits);
 
+/* Self-test of the bounded wait for the tensor cores' completion in the
+ * warm-start inference: one warpgroup allocates tensor memory, issues the
+ * layer-2 MMAs on zero operands and commits them (issue != 0) or issues
+ * nothing (issue == 0), and waits at most `spins` polls; *h_bits receives
+ * CANOE_EBIT_TIMEOUT if the wait gave up and CANOE_EBIT_NAN if a completed
+ * accumulator did not read back as zeros.  The tensor memory is freed in
+ * both cases.  No reference counterpart. */
+int canoe_selftest_umma_wait(int spins, int issue, uint32_t *h_bits);
+
 /* Measured non-tensor FMA throughput of the current GPU in TFLOP/s (2 flops
  * per FMA): FP64 (fp32 == 0) or FP32, eight independent chains per thread on
  * every SM, timed with CUDA events after a warm-up launch.  The denominator
