@@ -110,13 +110,26 @@ __global__ void __launch_bounds__(256)
       }
     }
   }
-  // warp reductions
+  // warp reductions, then one per CTA (256 threads): one atomic per CTA on
+  // the step's single dt accumulator instead of one per warp
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
     bits |= __shfl_xor_sync(0xffffffffu, bits, o);
   }
+  __shared__ double sdt[8];
+  __shared__ uint32_t sbits[8];
+  const int wid = threadIdx.x >> 5;
   if ((threadIdx.x & 31) == 0) {
+    sdt[wid] = dtc;
+    sbits[wid] = bits;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+      dtc = fmin(dtc, sdt[q]);
+      bits |= sbits[q];
+    }
     if (bits) atomicOr(err, bits);
     if (dt_acc && dtc < __longlong_as_double(0x7ff0000000000000LL)) atomicMin(dt_acc, dbits(dtc));
   }
