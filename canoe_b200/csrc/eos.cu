@@ -496,7 +496,21 @@ struct UmmaState {
   uint32_t phase;  // mbarrier phase of the next inference
   bool live;       // false once a bounded wait gave up: no further inference
   bool pending;    // the last inference's MMAs were not seen to complete
+  // this warp's statistics so far (cells, evaluations, fallbacks, not
+  // converged; the same on every lane), added to the global counters once
+  // per CTA or warp by the kernel rather than per chunk: every warp adding
+  // to the same four addresses serialised in L2
+  uint32_t acc[4];
 };
+
+// add a warp's (or CTA's) statistics to the global counters
+__device__ __forceinline__ void satadj_flush(unsigned long long *stats, const uint32_t *acc) {
+  if (!acc[0]) return;
+  atomicAdd(&stats[0], (unsigned long long)acc[0]);
+  atomicAdd(&stats[1], (unsigned long long)acc[1]);
+  if (acc[2]) atomicAdd(&stats[2], (unsigned long long)acc[2]);
+  if (acc[3]) atomicAdd(&stats[3], (unsigned long long)acc[3]);
+}
 
 // The network's inference as a call rather than inlined code: most warps of
 // a step never run it (no cell near saturation), and inlined it would hold
@@ -589,8 +603,8 @@ __device__ __forceinline__ void satadj_chunk(
     if (iters) iters[t] = it;
   }
   if (stats) {
-    unsigned long long a = active ? 1ull : 0ull, b = (unsigned long long)it,
-                       c = (fl & 1) ? 1ull : 0ull, d = (fl & 2) ? 1ull : 0ull;
+    uint32_t a = active ? 1u : 0u, b = (uint32_t)it, c = (fl & 1) ? 1u : 0u,
+             d = (fl & 2) ? 1u : 0u;
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
       a += __shfl_xor_sync(0xffffffffu, a, s);
@@ -598,12 +612,10 @@ __device__ __forceinline__ void satadj_chunk(
       c += __shfl_xor_sync(0xffffffffu, c, s);
       d += __shfl_xor_sync(0xffffffffu, d, s);
     }
-    if ((threadIdx.x & 31) == 0 && a) {
-      atomicAdd(&stats[0], a);
-      atomicAdd(&stats[1], b);
-      if (c) atomicAdd(&stats[2], c);
-      if (d) atomicAdd(&stats[3], d);
-    }
+    us.acc[0] += a;
+    us.acc[1] += b;
+    us.acc[2] += c;
+    us.acc[3] += d;
   }
 }
 
@@ -616,10 +628,13 @@ __global__ void __launch_bounds__(256, 3)
              int64_t ncells, int64_t stride, Geom g, int use_geom,
              const double *__restrict__ t_guess, double *__restrict__ t_out,
              int32_t *__restrict__ iters, unsigned long long *stats) {
-  UmmaState us{0u, false, false};
+  UmmaState us{0u, false, false, {0u, 0u, 0u, 0u}};
   satadj_chunk<NY, false>(th, o, u, ncells, stride, g, use_geom, t_guess, t_out, iters, stats,
                           MlpView{}, nullptr, nullptr,
                           (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nullptr, us, 0);
+  // one set of atomics per warp: a CTA-wide sum first (a barrier at the end)
+  // made C4's cold start slower (2.95 -> 3.07 ms)
+  if (stats && (threadIdx.x & 31) == 0) satadj_flush(stats, us.acc);
 }
 
 // the learned start: one persistent CTA of kSatWg warpgroups per SM (a
@@ -636,13 +651,14 @@ __global__ void __launch_bounds__(kSatWg * kUmmaM, 1)
                      double *__restrict__ guess_out, uint32_t *err) {
   extern __shared__ __align__(1024) uint8_t dsm[];
   mlp_umma_setup<kSatWg>(dsm, mv.p, mv.w2h);
-  UmmaState us{0u, true, false};
+  UmmaState us{0u, true, false, {0u, 0u, 0u, 0u}};
   const int wg = threadIdx.x / kUmmaM;
   const int64_t nchunk = (ncells + kUmmaM - 1) / kUmmaM;
   for (int64_t c = (int64_t)blockIdx.x * kSatWg + wg; c < nchunk;
        c += (int64_t)gridDim.x * kSatWg)
     satadj_chunk<NY, true>(th, o, u, ncells, stride, g, use_geom, t_guess, t_out, iters, stats,
                            mv, guess_out, err, c * kUmmaM + threadIdx.x % kUmmaM, dsm, us, wg);
+  if (stats && (threadIdx.x & 31) == 0) satadj_flush(stats, us.acc);
   mlp_umma_teardown<kSatWg>(dsm, us.pending, us.phase);
 }
 
